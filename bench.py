@@ -1,0 +1,345 @@
+"""Benchmark of the MPM substep: particle-substeps/s on one or more B200s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1]
+                    [--impl ours|reference]
+
+A step is one explicit MPM substep (P2G with stress, grid update, G2P with
+the F update and advection) over every particle of the workload, state
+resident in HBM.  The default workload is the 3D jello scene: 128^3 grid,
+0.3 cube at 8 particles/cell (~453k particles), E = 5e4, nu = 0.3,
+rho = 1000, dt = 1e-4, slip walls 3 cells wide; synthetic seeded particles
+(no dataset exists for this scene).
+
+Multi-GPU (torchrun, one process per GPU): every rank simulates its own
+replica of the workload (c1) or its share of the 64 batched scenes (c4); the
+path has no exchange step, so there is no data-path collective ("weak"
+scaling).  Timing: CUDA events on the simulation's stream around every
+substep, L2 flushed (256 MB write) between substeps outside the events,
+max over ranks.
+
+--impl reference runs the reference's own substep (MPMSimulator::step() of
+MPMCUDA.cu, built unmodified into oracle/_ref/libmpm_ref.so) on the same
+scene through its own code path (FP64 state, host syncs and a device-to-host
+position copy every substep).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-substeps/sec @1 B200, surrogate vs plain at stated stress/position error; HBM GB/s"
+UNIT = "particle-substeps/s"
+L2_FLUSH_BYTES = 256 << 20
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ helpers
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.idx), "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc or not self.path:
+            return None
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def build_workload(name: str, rank: int, world: int):
+    from mpm_cuda_b200 import scenes as S
+    if name == "c4":
+        all_scenes = S.c4_batched()
+        return [s for i, s in enumerate(all_scenes) if i % world == rank], "c4 64 batched scenes (jello/snow/water)"
+    if name == "c0":
+        return [S.c0_jello2d(seed=1234 + rank)], "c0 2D jello 128^2, 9000 particles"
+    if name == "c2":
+        return [S.c2_snow3d(seed=1234 + rank)], "c2 3D snow 256^3, two spheres r=0.12, 8 ppc"
+    if name == "c3":
+        return [S.c3_jello3d(seed=1234 + rank)], "c3 3D jello 256^3, 0.245 cube, 8 ppc"
+    if name == "c3big":
+        return [S.c3_jello3d(seed=1234 + rank, edge=0.45)], "c3 3D jello 256^3, 0.45 cube, 8 ppc"
+    return [S.c1_jello3d(seed=1234 + rank)], "c1 3D jello 128^3, 0.3 cube, 8 ppc"
+
+
+def state_bytes_per_particle(scenes):
+    """Algorithmic bytes of one particle's state, FP32: x v C F for solids
+    (+ det Fp for snow), x v C J for water."""
+    from mpm_cuda_b200 import _lib as L
+    tot, n = 0, 0
+    for s in scenes:
+        d = s.dim
+        for g in s.groups:
+            base = 4 * (2 * d + d * d)
+            per = base + 4 * d * d if g.material.type != L.WATER else base + 4
+            if g.material.type == L.SNOW:
+                per += 4
+            tot += per * g.n
+            n += g.n
+    return tot / max(n, 1)
+
+
+def cpu_baseline(scene, budget_s: float = 12.0):
+    """The FP64 oracle (OpenMP, all host cores) on the same scene."""
+    from oracle import cpu as ocpu
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import oracle_for
+    orc = oracle_for(scene)
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        orc.step(1, threads=cores)
+        steps += 1
+        if time.perf_counter() - t0 > budget_s or steps >= 50:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": scene.n_particles * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} substeps of the full {scene.name} scene ({scene.n_particles} particles), "
+                      f"FP64 C oracle, OpenMP {cores} threads, {dt:.1f} s"}
+
+
+# ----------------------------------------------------------------- our arm
+
+def run_ours(args, rank, world, local_rank, dist):
+    import torch
+    from mpm_cuda_b200.sim import Simulation
+
+    torch.cuda.set_device(local_rank)
+    scenes, desc = build_workload(args.workload, rank, world)
+    n_part = sum(s.n_particles for s in scenes)
+    sim = Simulation(scenes, device=local_rank)
+    stream = torch.cuda.ExternalStream(sim.stream_ptr(), device=local_rank)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
+
+    sim.step(args.warmup)
+    sim.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                starts[k].record(stream)
+                sim.step_async(1)
+                ends[k].record(stream)
+                flush.zero_()
+        sim.synchronize()
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    t_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    t = torch.tensor([t_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+    n_all = torch.tensor([float(n_part)], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(n_all, op=dist.ReduceOp.SUM)
+    t_max_s = float(t.item()) / 1e3
+    total_particles = float(n_all.item())
+    value = total_particles * args.steps / t_max_s
+    clocks = clk.summary()
+
+    # per-kernel device time (separate launches, CUDA events on the same stream)
+    stages = sim.profile_stages(20)
+    stage_names = ["p2g", "grid_update", "g2p"]
+    active_nodes = sum(sim.count_active_nodes(i) for i in range(len(scenes)))
+    sp = state_bytes_per_particle(scenes)
+    d = scenes[0].dim
+    x_f_bytes = 4 * (d + d * d)
+    alg = {"p2g": n_part * sp + active_nodes * 16,
+           "grid_update": active_nodes * 48,
+           "g2p": n_part * (x_f_bytes + sp) + active_nodes * 16}
+    dom = int(np.argmax(stages))
+    dom_name = stage_names[dom]
+    peak, peak_kind = hbm_peak()
+    achieved = alg[dom_name] / (stages[dom] * 1e-3) / 1e9
+    sub_bytes = n_part * 2 * sp + active_nodes * 64
+    roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes": int(alg[dom_name]),
+                "stage_ms": {n: round(s, 4) for n, s in zip(stage_names, stages)},
+                "substep_algorithmic_bytes": int(sub_bytes),
+                "substep_frac": round(sub_bytes / (t_max_s / args.steps) / 1e9 / peak, 4)}
+
+    # end to end through the public API: synchronous mpm_step + positions to host
+    e2e_steps = min(args.steps, 200)
+    pos = np.empty((n_part, d), np.float32)
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sim.step(1)
+        off = 0
+        for i, s in enumerate(scenes):
+            p = sim.positions(i)
+            pos[off:off + len(p)] = p
+            off += len(p)
+    e2e_t = time.perf_counter() - t0
+    e2e_t_t = torch.tensor([e2e_t], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if dist is not None:
+        dist.all_reduce(e2e_t_t, op=dist.ReduceOp.MAX)
+    e2e = {"value": total_particles * e2e_steps / float(e2e_t_t.item()), "unit": UNIT,
+           "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(n_part * d * 4),
+           "how": "mpm_step(h, 1) then mpm_get_positions into host memory every substep, wall clock "
+                  "(the reference's loop: step() copies positions to the host every substep); "
+                  "state stays resident in HBM between substeps as in the reference"}
+    sim.close()
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max_s * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": desc, "particles_per_gpu": n_part, "particles_total": int(total_particles),
+                       "active_nodes": active_nodes, "stress": "plain (SVD)", "p2g": "atomic",
+                       "l2": "flushed between substeps (256 MB write, outside the timed events)",
+                       "parallelism": f"replicas x{world}" if args.workload != "c4" else f"scenes split over {world}"},
+            "roofline": roofline, "e2e": e2e, "gpu_launches": 3 * args.steps, "clocks": clocks}
+    return line, scenes
+
+
+# ----------------------------------------------------------- reference arm
+
+def run_reference(args):
+    from oracle import ref as R
+    if not R.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libmpm_ref.so was not built (needs the reference tree)"}
+    scenes, desc = build_workload("c1" if args.workload not in ("c1", "c3", "c2") else args.workload, 0, 1)
+    sc = scenes[0]
+    sim = R.RefSim(sc.h, sc.dt, sc.n)
+    for g in sc.groups:
+        m = g.material
+        n = g.n
+        x = np.float64(g.x)
+        v = np.tile(np.float64(g.init_v[:3]), (n, 1))
+        F = np.tile(np.eye(3), (n, 1, 1))
+        Fp = np.tile(np.eye(3), (n, 1, 1)) if m.type == 1 else None
+        J = np.ones(n) if m.type == 2 else None
+        sim.add_group(m.type, m.E if m.type != 2 else 1e4, m.nu if m.type != 2 else 0.2, m.rho, g.p_mass,
+                      g.p_vol, x, v, F, Fp=Fp, J=J, C_=np.zeros((n, 3, 3)))
+    steps = min(args.steps, 200)
+    warm = min(args.warmup, 20)
+    sim.step(warm)
+    ms = sim.time_steps(steps)
+    sim.close()
+    n = sc.n_particles
+    value = n * steps / (ms * 1e-3)
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps,
+            "warmup": warm, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": desc, "particles_per_gpu": n,
+                       "note": "reference MPMSimulator::step() (MPMCUDA.cu:793-925) built unmodified for sm_100a; "
+                               "its stock path: FP64 state, 3 device syncs and a D2H position copy per substep; "
+                               "its hard-coded 10h walls and constants"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": f"{steps} substeps of {desc}; the reference implementation of this path "
+                                       "is CUDA, so it runs on the B200 driven by one host thread"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--workload", default="c1", choices=["c0", "c1", "c2", "c3", "c3big", "c4"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference(args)), flush=True)
+        return 0
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device(f"cuda:{local_rank}"))
+        dist = tdist
+    line, scenes = run_ours(args, rank, world, local_rank, dist)
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(scenes[0])
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,217 @@
+/*
+ * mpm_b200.h -- C ABI of the B200-native explicit MPM substep.
+ *
+ * This is the drop-in boundary for the substep loop of the reference
+ * simulator (JerryYan97/MPM_CUDA).  Each entry point names the reference
+ * interface it replaces (path:line within the reference project).  The
+ * reference exposes a C++ class; the C++ class with the reference's exact
+ * signatures lives in mpm_simulator.hpp and forwards here.
+ *
+ * Conventions
+ *   - Every function returns an int status (MPM_OK = 0, negative on error)
+ *     and never calls exit() or throws across the ABI (the reference calls
+ *     exit(1) on any CUDA error, e.g. MPMSimulator.cpp:36-39).
+ *   - Host arrays are plain float / double pointers with explicit sizes.
+ *   - A handle owns all device memory and one CUDA stream.  A handle is not
+ *     thread-safe: use one handle per host thread.
+ *   - Particle arrays passed across the ABI are per-particle interleaved
+ *     (AoS): x[N*dim], v[N*dim], C[N*dim*dim], F[N*dim*dim] (row-major
+ *     matrices), aux[N].  aux is det(Fp) for snow, J for water, unused (1)
+ *     for jello.
+ */
+#ifndef MPM_B200_H
+#define MPM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPM_ABI_VERSION 1
+
+/* Material types; values match the reference enum MaterialType
+ * (src/simulator/material/Elasiticity.cuh:10-11).  SAND is declared there but
+ * has no implementation (MPMCUDA.cu:415-416); mpm_create rejects it. */
+enum mpm_material_type { MPM_JELLO = 0, MPM_SNOW = 1, MPM_WATER = 2, MPM_SAND = 3 };
+
+/* Wall treatment of the grid update (VelUpdate, MPMCUDA.cu:459-469).
+ * A node with index i along an axis is a lower-wall node if i < bc_lo and an
+ * upper-wall node if i >= n - bc_hi.  The reference 3D build corresponds to
+ * MPM_BC_SLIP with bc_lo = 11, bc_hi = 10 (its 10h band, MPMCUDA.cu:845-850). */
+enum mpm_boundary_type {
+    MPM_BC_STICKY = 0,   /* zero all velocity components of a wall node */
+    MPM_BC_SLIP = 1,     /* zero the wall-normal component */
+    MPM_BC_SEPARATE = 2  /* zero the wall-normal component only when moving
+                            into the wall (MPMJello.py:92-95) */
+};
+
+/* P2G reduction modes */
+enum mpm_p2g_mode {
+    MPM_P2G_ATOMIC = 0,        /* shared-memory staged FP32 atomics (fast;
+                                  summation order varies run to run) */
+    MPM_P2G_DETERMINISTIC = 1  /* sorted gather reduction: bitwise identical
+                                  results across runs */
+};
+
+/* Stress evaluation modes */
+enum mpm_stress_mode {
+    MPM_STRESS_PLAIN = 0,     /* 3x3 SVD fixed-corotated stress */
+    MPM_STRESS_SURROGATE = 1  /* learned MLP stress with SVD fallback */
+};
+
+/* Status codes */
+enum mpm_status {
+    MPM_OK = 0,
+    MPM_ERR_INVALID = -1,     /* bad argument or descriptor */
+    MPM_ERR_CUDA = -2,        /* CUDA runtime error (text in mpm_last_error) */
+    MPM_ERR_NOMEM = -3,       /* device allocation failed */
+    MPM_ERR_UNSUPPORTED = -4, /* valid but not implemented (e.g. SAND) */
+    MPM_ERR_SIM = -5,         /* the device error word is non-zero */
+    MPM_ERR_IO = -6           /* file output failed */
+};
+
+/* Bits of the device error word (replace the reference's device asserts,
+ * MPMCUDA.cu:376-386,431,546,614,702,725-739). */
+enum mpm_device_error {
+    MPM_DEVERR_OUT_OF_GRID = 1, /* a particle's stencil left its grid */
+    MPM_DEVERR_NONFINITE = 2,   /* NaN or Inf in particle state */
+    MPM_DEVERR_DET = 4,         /* det F <= 0, det Fp <= 0 or J <= 0 */
+    MPM_DEVERR_TIMEOUT = 16     /* a bounded device-side wait gave up */
+};
+
+typedef struct mpm_material_desc {
+    int type;       /* enum mpm_material_type */
+    double E, nu;   /* Young's modulus, Poisson ratio -> Lame parameters as
+                       Material(E, nu, rho, type), Elasiticity.cuh:30-45 */
+    double rho;     /* density (informational; mass comes from p_mass) */
+    double xi;      /* snow hardening, mu,lambda *= exp(xi (1 - Jp));
+                       reference 10 (MPMCUDA.cu:344) */
+    double theta_c; /* snow: sigma clamped to >= 1 - theta_c; reference 8e-2
+                       (MPMCUDA.cu:658-660) */
+    double theta_s; /* snow: sigma clamped to <= 1 + theta_s; reference 2e-2 */
+    double bulk_k;  /* water: p = bulk_k (J^-gamma - 1); reference 2.51
+                       (MPMCUDA.cu:353) */
+    double gamma;   /* water exponent; reference 7 */
+} mpm_material_desc;
+
+/* One particle group (the reference's ParticleGroup, MPMSimulator.cuh:30-52). */
+typedef struct mpm_group_desc {
+    mpm_material_desc material;
+    double p_mass, p_vol;  /* per-particle mass and initial volume */
+    int64_t n;             /* number of particles */
+    const float *x;        /* [n*dim] positions (required) */
+    const float *v;        /* [n*dim] velocities, or NULL -> init_v */
+    double init_v[3];
+    const float *F;        /* [n*dim*dim] or NULL -> identity */
+    const float *C;        /* [n*dim*dim] or NULL -> zero */
+    const float *aux;      /* [n] Jp (snow) / J (water), or NULL -> 1 */
+} mpm_group_desc;
+
+/* One scene: a grid plus its particle groups (the reference's Grid,
+ * MPMSimulator.cuh:54-64, and simulator scalars). */
+typedef struct mpm_scene_desc {
+    int dim;           /* 2 or 3 */
+    int n[3];          /* grid nodes per axis; n[2] = 1 for dim 2 */
+    double h;          /* node spacing (the reference's `gap`) */
+    double origin[3];  /* grid corner (the reference uses 0) */
+    double dt;         /* substep (the reference's adp_dt = max_dt) */
+    double gravity[3]; /* the reference adds -9.8 to y (MPMSimulator.cpp:186) */
+    int bc_type, bc_lo, bc_hi;
+    double mass_eps;   /* nodes with mass <= mass_eps get zero velocity;
+                          reference DBL_EPSILON (MPMCUDA.cu:444) */
+    int n_groups;
+    const mpm_group_desc *groups;
+} mpm_scene_desc;
+
+typedef struct mpm_options {
+    int p2g_mode;     /* enum mpm_p2g_mode */
+    int stress_mode;  /* enum mpm_stress_mode */
+    int use_graph;    /* capture the substep in a CUDA graph (default 1) */
+    int block_threads;/* threads per CTA for particle kernels; 0 = tuned */
+    int device;       /* CUDA device ordinal */
+} mpm_options;
+
+typedef struct mpm_handle mpm_handle;
+
+/* Fills *opt with defaults (ATOMIC, PLAIN, graphs on, tuned sizes, device 0). */
+void mpm_default_options(mpm_options *opt);
+
+/* Replaces MPMSimulator::MPMSimulator(gap, dt, nx, ny, nz, ppc, objs)
+ * (src/simulator/MPMSimulator.cuh:92-96, MPMSimulator.cpp:178-285): builds
+ * n_scenes independent scenes on one device.  opt may be NULL. */
+int mpm_create(const mpm_scene_desc *scenes, int n_scenes, const mpm_options *opt,
+               mpm_handle **out);
+
+/* Replaces ~MPMSimulator() (MPMSimulator.cuh:101, MPMSimulator.cpp:288-352). */
+int mpm_destroy(mpm_handle *h);
+
+/* Replaces MPMSimulator::step() (MPMSimulator.cuh:98, MPMCUDA.cu:793-925):
+ * advances every scene by n_substeps and waits for completion; returns
+ * MPM_ERR_SIM if the device error word became non-zero. */
+int mpm_step(mpm_handle *h, int n_substeps);
+
+/* Same as mpm_step but returns right after enqueueing on the handle's
+ * stream; call mpm_synchronize to wait and collect the error word. */
+int mpm_step_async(mpm_handle *h, int n_substeps);
+int mpm_synchronize(mpm_handle *h);
+
+/* Device error word (enum mpm_device_error bits), read after a sync. */
+int mpm_get_device_errors(mpm_handle *h, uint32_t *bits);
+int mpm_clear_device_errors(mpm_handle *h);
+
+/* The handle's CUDA stream (a cudaStream_t) for event timing. */
+int mpm_get_stream(mpm_handle *h, void **stream);
+
+/* Replaces MPMSimulator::totalParticlesNum() (MPMSimulator.cuh:99):
+ * scene < 0 counts every scene. */
+int mpm_num_particles(mpm_handle *h, int scene, int64_t *n);
+
+/* Replaces MPMSimulator::getGLParticlesPos(std::vector<float>&)
+ * (MPMSimulator.cuh:100, MPMSimulator.cpp:362-371): copies a scene's
+ * positions, in creation order, as float x[N*dim].  cap is in floats. */
+int mpm_get_positions(mpm_handle *h, int scene, float *host_out, size_t cap);
+
+/* Full particle state of one scene in creation order (the reference's device
+ * arrays, MPMSimulator.cuh:37-43).  Any pointer may be NULL to skip it. */
+int mpm_get_state(mpm_handle *h, int scene, float *x, float *v, float *C, float *F,
+                  float *aux);
+int mpm_set_state(mpm_handle *h, int scene, const float *x, const float *v,
+                  const float *C, const float *F, const float *aux);
+
+/* Grid of one scene after the last grid update: mass[G] and velocity
+ * vel[G*dim], x-fastest node order as MPMCUDA.cu:375.  Either may be NULL. */
+int mpm_get_grid(mpm_handle *h, int scene, float *mass, float *vel);
+
+/* Simulated time and substep count of a scene (the reference's public
+ * current_time / current_frame, MPMSimulator.cuh:86-87). */
+int mpm_get_time(mpm_handle *h, double *current_time, int64_t *current_frame);
+
+/* Replaces OutputBego(path, positions) (src/utilities/FilesIO.h:10,
+ * FilesIO.cpp:6-24): writes the scene's positions as a Houdini .bgeo
+ * particle file with one float[3] "position" attribute. */
+int mpm_write_bgeo(mpm_handle *h, int scene, const char *path);
+
+/* Writes host positions (x[n*3]) as .bgeo without a handle. */
+int mpm_write_bgeo_positions(const char *path, const float *x, int64_t n);
+
+/* Switches the P2G reduction mode (enum mpm_p2g_mode) of a live handle. */
+int mpm_set_p2g_mode(mpm_handle *h, int mode);
+
+/* Last error message of the handle (or of the thread when h is NULL). */
+int mpm_last_error(mpm_handle *h, char *buf, size_t cap);
+
+/* Per-stage device time of one substep, measured with CUDA events on the
+ * handle's stream, averaged over n_substeps: out_ms[0..n_out) in stage order
+ * (bin, p2g, grid_update, g2p).  Writes the stage names count to *n_written. */
+int mpm_profile_stages(mpm_handle *h, int n_substeps, float *out_ms, int n_out,
+                       int *n_written);
+
+/* Number of grid nodes with non-zero mass in one scene after the last step. */
+int mpm_count_active_nodes(mpm_handle *h, int scene, int64_t *n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPM_B200_H */

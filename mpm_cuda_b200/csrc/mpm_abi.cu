@@ -1,0 +1,210 @@
+// C-ABI of the B200 MPM substep (declared in include/mpm_b200.h).
+//
+// A handle owns: the particle state of every scene (FP32 component planes,
+// all scenes concatenated), the per-scene blocked grids, the group/scene
+// parameter tables, a CUDA stream and the CUDA graph of one substep.
+#include "mpm_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "mpm_engine.cuh"
+
+namespace {
+
+thread_local std::string g_thread_error;
+
+}  // namespace
+
+using mpm::Engine;
+
+struct mpm_handle {
+    Engine eng;
+};
+
+static int fail(mpm_handle* h, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (h) h->eng.last_error = buf;
+    else g_thread_error = buf;
+    return code;
+}
+
+extern "C" {
+
+void mpm_default_options(mpm_options* opt) {
+    if (!opt) return;
+    opt->p2g_mode = MPM_P2G_ATOMIC;
+    opt->stress_mode = MPM_STRESS_PLAIN;
+    opt->use_graph = 1;
+    opt->block_threads = 0;
+    opt->device = 0;
+}
+
+int mpm_create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options* opt,
+               mpm_handle** out) {
+    if (!out) return fail(nullptr, MPM_ERR_INVALID, "mpm_create: out is NULL");
+    *out = nullptr;
+    mpm_options o;
+    mpm_default_options(&o);
+    if (opt) o = *opt;
+    auto* h = new (std::nothrow) mpm_handle();
+    if (!h) return fail(nullptr, MPM_ERR_NOMEM, "mpm_create: host allocation failed");
+    std::string msg;
+    int rc = h->eng.create(scenes, n_scenes, o, msg);
+    if (rc != MPM_OK) {
+        g_thread_error = msg;
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return MPM_OK;
+}
+
+int mpm_destroy(mpm_handle* h) {
+    if (!h) return MPM_OK;
+    h->eng.release();
+    delete h;
+    return MPM_OK;
+}
+
+int mpm_step(mpm_handle* h, int n) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_step: NULL handle");
+    int rc = h->eng.step(n);
+    if (rc != MPM_OK) return rc;
+    return h->eng.sync_and_check();
+}
+
+int mpm_step_async(mpm_handle* h, int n) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_step_async: NULL handle");
+    return h->eng.step(n);
+}
+
+int mpm_synchronize(mpm_handle* h) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_synchronize: NULL handle");
+    return h->eng.sync_and_check();
+}
+
+int mpm_get_device_errors(mpm_handle* h, uint32_t* bits) {
+    if (!h || !bits) return fail(h, MPM_ERR_INVALID, "mpm_get_device_errors: bad argument");
+    return h->eng.read_errors(bits);
+}
+
+int mpm_clear_device_errors(mpm_handle* h) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_clear_device_errors: NULL handle");
+    return h->eng.clear_errors();
+}
+
+int mpm_get_stream(mpm_handle* h, void** stream) {
+    if (!h || !stream) return fail(h, MPM_ERR_INVALID, "mpm_get_stream: bad argument");
+    *stream = (void*)h->eng.stream;
+    return MPM_OK;
+}
+
+int mpm_num_particles(mpm_handle* h, int scene, int64_t* n) {
+    if (!h || !n) return fail(h, MPM_ERR_INVALID, "mpm_num_particles: bad argument");
+    if (scene < 0) {
+        *n = h->eng.n_particles;
+        return MPM_OK;
+    }
+    if (scene >= (int)h->eng.scenes_h.size())
+        return fail(h, MPM_ERR_INVALID, "mpm_num_particles: scene %d out of range", scene);
+    *n = h->eng.scene_count[scene];
+    return MPM_OK;
+}
+
+int mpm_get_positions(mpm_handle* h, int scene, float* x, size_t cap) {
+    if (!h || !x) return fail(h, MPM_ERR_INVALID, "mpm_get_positions: bad argument");
+    if (scene < 0 || scene >= (int)h->eng.scenes_h.size())
+        return fail(h, MPM_ERR_INVALID, "mpm_get_positions: scene %d out of range", scene);
+    size_t need = (size_t)h->eng.scene_count[scene] * h->eng.dim;
+    if (cap < need)
+        return fail(h, MPM_ERR_INVALID, "mpm_get_positions: cap %zu < %zu floats", cap, need);
+    return h->eng.get_state(scene, x, nullptr, nullptr, nullptr, nullptr);
+}
+
+int mpm_get_state(mpm_handle* h, int scene, float* x, float* v, float* C, float* F, float* aux) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_get_state: NULL handle");
+    if (scene < 0 || scene >= (int)h->eng.scenes_h.size())
+        return fail(h, MPM_ERR_INVALID, "mpm_get_state: scene %d out of range", scene);
+    return h->eng.get_state(scene, x, v, C, F, aux);
+}
+
+int mpm_set_state(mpm_handle* h, int scene, const float* x, const float* v, const float* C,
+                  const float* F, const float* aux) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_set_state: NULL handle");
+    if (scene < 0 || scene >= (int)h->eng.scenes_h.size())
+        return fail(h, MPM_ERR_INVALID, "mpm_set_state: scene %d out of range", scene);
+    return h->eng.set_state(scene, x, v, C, F, aux);
+}
+
+int mpm_get_grid(mpm_handle* h, int scene, float* mass, float* vel) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_get_grid: NULL handle");
+    if (scene < 0 || scene >= (int)h->eng.scenes_h.size())
+        return fail(h, MPM_ERR_INVALID, "mpm_get_grid: scene %d out of range", scene);
+    return h->eng.get_grid(scene, mass, vel);
+}
+
+int mpm_count_active_nodes(mpm_handle* h, int scene, int64_t* n) {
+    if (!h || !n) return fail(h, MPM_ERR_INVALID, "mpm_count_active_nodes: bad argument");
+    if (scene < 0 || scene >= (int)h->eng.scenes_h.size())
+        return fail(h, MPM_ERR_INVALID, "mpm_count_active_nodes: scene %d out of range", scene);
+    return h->eng.count_active_nodes(scene, n);
+}
+
+int mpm_get_time(mpm_handle* h, double* t, int64_t* frame) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_get_time: NULL handle");
+    if (t) *t = h->eng.current_time;
+    if (frame) *frame = h->eng.current_frame;
+    return MPM_OK;
+}
+
+int mpm_write_bgeo(mpm_handle* h, int scene, const char* path) {
+    if (!h || !path) return fail(h, MPM_ERR_INVALID, "mpm_write_bgeo: bad argument");
+    if (scene < 0 || scene >= (int)h->eng.scenes_h.size())
+        return fail(h, MPM_ERR_INVALID, "mpm_write_bgeo: scene %d out of range", scene);
+    std::vector<float> x((size_t)h->eng.scene_count[scene] * h->eng.dim);
+    int rc = h->eng.get_state(scene, x.data(), nullptr, nullptr, nullptr, nullptr);
+    if (rc != MPM_OK) return rc;
+    if (mpm::write_bgeo(path, x.data(), h->eng.scene_count[scene], h->eng.dim) != 0)
+        return fail(h, MPM_ERR_IO, "mpm_write_bgeo: cannot write %s", path);
+    return MPM_OK;
+}
+
+int mpm_write_bgeo_positions(const char* path, const float* x, int64_t n) {
+    if (mpm::write_bgeo(path, x, n, 3) != 0)
+        return fail(nullptr, MPM_ERR_IO, "mpm_write_bgeo_positions: cannot write %s",
+                    path ? path : "(null)");
+    return MPM_OK;
+}
+
+int mpm_set_p2g_mode(mpm_handle* h, int mode) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_set_p2g_mode: NULL handle");
+    if (mode != MPM_P2G_ATOMIC && mode != MPM_P2G_DETERMINISTIC)
+        return fail(h, MPM_ERR_INVALID, "mpm_set_p2g_mode: bad mode %d", mode);
+    return h->eng.set_p2g_mode(mode);
+}
+
+int mpm_last_error(mpm_handle* h, char* buf, size_t cap) {
+    if (!buf || cap == 0) return MPM_ERR_INVALID;
+    const std::string& s = h ? h->eng.last_error : g_thread_error;
+    std::snprintf(buf, cap, "%s", s.c_str());
+    return MPM_OK;
+}
+
+int mpm_profile_stages(mpm_handle* h, int n, float* out_ms, int n_out, int* n_written) {
+    if (!h || !out_ms || n <= 0) return fail(h, MPM_ERR_INVALID, "mpm_profile_stages: bad argument");
+    return h->eng.profile_stages(n, out_ms, n_out, n_written);
+}
+
+}  // extern "C"

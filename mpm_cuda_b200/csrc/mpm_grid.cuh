@@ -1,0 +1,92 @@
+// Grid layout and the grid update.
+//
+// Each scene owns a dense grid stored in 64-node blocks: 4x4x4 nodes in 3D,
+// 8x8 nodes in 2D.  A node is one float4: (momentum or velocity xyz, mass).
+// Blocks of a scene are x-fastest; nodes inside a block are x-fastest.  The
+// blocked order keeps a stencil, a shared-memory tile and a grid-update CTA
+// on a few contiguous 1 KB runs.
+#pragma once
+
+#include "mpm_types.cuh"
+
+namespace mpm {
+
+template <int D>
+struct BlockShape {
+    static constexpr int SIDE = (D == 3) ? 4 : 8;
+    static constexpr int SHIFT = (D == 3) ? 2 : 3;
+    static constexpr int NODES = 64;
+};
+
+template <int D>
+__device__ __forceinline__ long long node_index(const SceneParams& sc, int ix, int iy, int iz) {
+    constexpr int S = BlockShape<D>::SHIFT;
+    constexpr int M = BlockShape<D>::SIDE - 1;
+    long long blk = (long long)(ix >> S) + (long long)sc.nb[0] * ((iy >> S) + (long long)sc.nb[1] * (iz >> S));
+    int in = (ix & M) + BlockShape<D>::SIDE * ((iy & M) + BlockShape<D>::SIDE * (iz & M));
+    return sc.node_off + blk * 64 + in;
+}
+
+// scene owning global block `b` (binary search over block_off)
+__device__ __forceinline__ int scene_of_block(const SceneParams* scenes, int n_scenes, long long b) {
+    int lo = 0, hi = n_scenes - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (scenes[mid].block_off <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Grid update of one node (VelUpdate, MPMCUDA.cu:435-472): momentum to
+// velocity when mass > mass_eps, gravity, wall boundary.  `g` holds
+// (momentum, mass) on entry and (velocity, mass) on return.
+template <int D>
+__device__ __forceinline__ float4 grid_node_update(float4 g, const SceneParams& sc, int ix, int iy,
+                                                   int iz) {
+    const float m = g.w;
+    if (!(m > sc.mass_eps)) return make_float4(0.f, 0.f, 0.f, 0.f);
+    const float im = 1.f / m;
+    float v[3] = {fmaf(g.x, im, 0.f), fmaf(g.y, im, 0.f), fmaf(g.z, im, 0.f)};
+#pragma unroll
+    for (int a = 0; a < D; ++a) v[a] = fmaf(sc.dt, sc.gravity[a], v[a]);
+    const int id[3] = {ix, iy, iz};
+    bool lo[3], hi[3], any = false;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        lo[a] = id[a] < sc.bc_lo;
+        hi[a] = id[a] >= sc.n[a] - sc.bc_hi;
+        any |= lo[a] | hi[a];
+    }
+    if (sc.bc_type == BC_STICKY) {
+        if (any) v[0] = v[1] = v[2] = 0.f;
+    } else if (sc.bc_type == BC_SLIP) {
+#pragma unroll
+        for (int a = 0; a < D; ++a)
+            if (lo[a] || hi[a]) v[a] = 0.f;
+    } else {
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            if (lo[a] && v[a] < 0.f) v[a] = 0.f;
+            if (hi[a] && v[a] > 0.f) v[a] = 0.f;
+        }
+    }
+    if (D == 2) v[2] = 0.f;
+    return make_float4(v[0], v[1], v[2], m);
+}
+
+// coordinates of node `in` (0..63) of block `blk` of scene `sc`
+template <int D>
+__device__ __forceinline__ void block_node_coords(const SceneParams& sc, long long blk, int in, int& ix,
+                                                  int& iy, int& iz) {
+    constexpr int S = BlockShape<D>::SIDE;
+    const int bx = (int)(blk % sc.nb[0]);
+    const long long r = blk / sc.nb[0];
+    const int by = (int)(r % sc.nb[1]);
+    const int bz = (int)(r / sc.nb[1]);
+    ix = bx * S + (in % S);
+    iy = by * S + ((in / S) % S);
+    iz = (D == 3) ? bz * S + in / (S * S) : 0;
+}
+
+}  // namespace mpm

@@ -1,0 +1,68 @@
+// Device-side descriptors shared by the kernels and the C-ABI layer.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mpm {
+
+// material type values match the reference enum (Elasiticity.cuh:10-11)
+enum : int { JELLO = 0, SNOW = 1, WATER = 2, SAND = 3 };
+enum : int { BC_STICKY = 0, BC_SLIP = 1, BC_SEPARATE = 2 };
+enum : unsigned { ERR_OUT_OF_GRID = 1u, ERR_NONFINITE = 2u, ERR_DET = 4u, ERR_TIMEOUT = 16u };
+
+// One particle group: material + per-particle mass/volume (ParticleGroup,
+// MPMSimulator.cuh:30-52; Material, Elasiticity.cuh:19-45).
+struct GroupParams {
+    int scene;
+    int type;
+    float mu, lambda;
+    float xi, theta_c, theta_s;
+    float bulk_k, gamma;
+    float p_mass, p_vol;
+    int pad;
+};
+
+// One scene's grid and integration constants (Grid, MPMSimulator.cuh:54-64).
+struct SceneParams {
+    int n[3];
+    int dim;
+    float h, inv_h;
+    float origin[3];
+    float dt;
+    float gravity[3];
+    int bc_type, bc_lo, bc_hi;
+    float mass_eps;
+    long long node_off;  // first node of the scene in the global grid arrays
+    long long n_nodes;
+    // 4^3 (or 4^2) node blocks: blocks per axis and first block index
+    int nb[3];
+    int pad;
+    long long block_off;
+    long long n_blocks;
+};
+
+// Particle state: component planes of one FP32 buffer, plane stride `cap`.
+//   planes [0, D)              x
+//   planes [D, 2D)             v
+//   planes [2D, 2D + D^2)      C (row-major)
+//   planes [2D + D^2, 2D+2D^2) F (row-major)
+//   plane  2D + 2D^2           aux: det Fp (snow) / J (water)
+template <int D>
+struct Planes {
+    static constexpr int X = 0;
+    static constexpr int V = D;
+    static constexpr int C = 2 * D;
+    static constexpr int F = 2 * D + D * D;
+    static constexpr int AUX = 2 * D + 2 * D * D;
+    static constexpr int COUNT = 2 * D + 2 * D * D + 1;
+};
+
+struct ParticleBuf {
+    float* s;          // COUNT planes
+    long long cap;     // plane stride (elements)
+    uint16_t* grp;     // group index per particle
+    uint32_t* id;      // creation index per particle
+};
+
+}  // namespace mpm

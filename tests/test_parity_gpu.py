@@ -1,0 +1,222 @@
+"""GPU parity of the CUDA substep (through the C ABI) against the FP64 CPU
+oracle and the reference build's golden fixtures."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from mpm_cuda_b200 import _lib as L
+from mpm_cuda_b200 import scenes as S
+from mpm_cuda_b200.sim import Scene, Simulation
+
+from helpers import TOL_STEP, compare, group_from_arrays, oracle_for, rel_err
+
+pytestmark = pytest.mark.gpu
+
+MATS = {"jello": S.jello(), "snow": S.snow(), "water": S.water()}
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def blob_scene(d, name, bc=L.BC_SLIP, seed=3, n_grid=32, h=1.0 / 32, ppc=2, radius=5.0, **kw):
+    mat = MATS[name]
+    x, v, C, F, aux = S.perturbed_blob(d, mat, n_grid=n_grid, h=h, ppc=ppc, radius_cells=radius, seed=seed,
+                                       center=np.full(d, n_grid / 2 * h))
+    g = group_from_arrays(mat, h, ppc, x, v, C, F, aux)
+    return Scene(dim=d, n=(n_grid,) * d, h=h, dt=1e-4, groups=[g], bc_type=bc, bc_lo=3, bc_hi=3,
+                 gravity=(0.0, -9.8, 0.0)[:d] if d == 3 else (0.0, -9.8), **kw)
+
+
+@pytest.mark.parametrize("d", [2, 3])
+@pytest.mark.parametrize("name", ["jello", "snow", "water"])
+def test_one_substep_matches_oracle(gpu, d, name):
+    sc = blob_scene(d, name)
+    orc = oracle_for(sc)
+    with Simulation([sc]) as sim:
+        sim.step(1)
+        got = sim.get_state(0)
+    assert orc.step(1) == 0
+    compare(got, orc.state(), TOL_STEP)
+
+
+@pytest.mark.parametrize("d", [2, 3])
+@pytest.mark.parametrize("bc", [L.BC_STICKY, L.BC_SLIP, L.BC_SEPARATE])
+def test_boundaries_match_oracle(gpu, d, bc):
+    # blob pushed into the lower x wall band so every boundary branch runs
+    sc = blob_scene(d, "jello", bc=bc, seed=4)
+    g = sc.groups[0]
+    g.x[:, 0] -= np.float32(10 * sc.h)
+    g.v[:, 0] = -np.abs(g.v[:, 0]) - 1.0
+    sc.bc_lo, sc.bc_hi = 8, 3
+    orc = oracle_for(sc)
+    with Simulation([sc]) as sim:
+        sim.step(1)
+        got = sim.get_state(0)
+        mass, vel = sim.get_grid(0)
+    assert orc.step(1) == 0
+    compare(got, orc.state(), TOL_STEP)
+    ref_vel = orc.mom.reshape(-1, 3)[:, :d]
+    assert rel_err(vel, ref_vel) < 1e-4
+    assert rel_err(mass, orc.mass) < 1e-5
+
+
+def test_grid_matches_oracle(gpu):
+    sc = blob_scene(3, "snow", seed=8)
+    orc = oracle_for(sc)
+    with Simulation([sc]) as sim:
+        sim.step(1)
+        mass, vel = sim.get_grid(0)
+        active = sim.count_active_nodes(0)
+    orc.step(1)
+    assert rel_err(mass, orc.mass) < 1e-5
+    assert rel_err(vel, orc.mom.reshape(-1, 3)) < 1e-4
+    assert active == int((orc.mass > 0).sum())
+
+
+@pytest.mark.parametrize("name", ["jello", "snow", "water"])
+def test_twenty_substeps_track_oracle(gpu, name):
+    sc = blob_scene(3, name, seed=21)
+    orc = oracle_for(sc)
+    with Simulation([sc]) as sim:
+        sim.step(20)
+        got = sim.get_state(0)
+    assert orc.step(20) == 0
+    tol = {"x": 1e-5, "v": 2e-3, "C": 2e-3, "F": 1e-4, "aux": 1e-4}
+    compare(got, orc.state(), tol)
+
+
+def test_multi_scene_batch_matches_single(gpu):
+    scs = [blob_scene(3, "jello", seed=30), blob_scene(3, "snow", seed=31, n_grid=40, h=1.0 / 40),
+           blob_scene(3, "water", seed=32, n_grid=24, h=1.0 / 24)]
+    with Simulation(scs) as sim:
+        sim.step(3)
+        batched = [sim.get_state(i) for i in range(3)]
+    for i, sc in enumerate(scs):
+        orc = oracle_for(sc)
+        assert orc.step(3) == 0
+        compare(batched[i], orc.state(), {"x": 5e-6, "v": 5e-4, "C": 5e-4, "F": 3e-5, "aux": 3e-5})
+
+
+def test_mixed_groups_in_one_grid(gpu):
+    a = blob_scene(3, "jello", seed=40)
+    b = blob_scene(3, "water", seed=41)
+    for g in b.groups:
+        g.x[:, 0] += np.float32(3 * a.h)
+    a.groups += b.groups
+    orc = oracle_for(a)
+    with Simulation([a]) as sim:
+        sim.step(2)
+        got = sim.get_state(0)
+    assert orc.step(2) == 0
+    compare(got, orc.state(), {"x": 5e-6, "v": 3e-4, "C": 3e-4, "F": 2e-5, "aux": 2e-5})
+
+
+def test_graph_and_stream_paths_agree(gpu):
+    sc = blob_scene(3, "jello", seed=50)
+    with Simulation([sc], use_graph=True) as a, Simulation([sc], use_graph=False) as b:
+        a.step(5)
+        b.step(5)
+        sa, sb = a.get_state(0), b.get_state(0)
+    for k in ("x", "v", "C", "F"):
+        assert rel_err(sa[k], sb[k]) < 1e-5
+
+
+def test_set_get_state_roundtrip(gpu):
+    sc = blob_scene(3, "snow", seed=60)
+    with Simulation([sc]) as sim:
+        st = sim.get_state(0)
+        g = sc.groups[0]
+        assert np.array_equal(st["x"], g.x)
+        assert np.array_equal(st["F"], g.F)
+        st["x"][:, 1] += np.float32(0.01)
+        sim.set_state(0, x=st["x"])
+        st2 = sim.get_state(0)
+        assert np.array_equal(st2["x"], st["x"])
+        assert np.array_equal(st2["C"], g.C)
+        assert np.array_equal(sim.positions(0), st["x"])
+
+
+def test_out_of_grid_particle_sets_error_word(gpu):
+    sc = blob_scene(3, "jello", seed=70)
+    sc.groups[0].x[0] = np.float32([0.995, 0.5, 0.5])
+    with Simulation([sc]) as sim:
+        rc = sim.step_status(1)
+        assert rc == L.ERR_SIM
+        assert sim.device_errors() & L.DEVERR_OUT_OF_GRID
+        sim.clear_device_errors()
+        assert sim.device_errors() == 0
+
+
+def test_nan_particle_sets_error_word(gpu):
+    sc = blob_scene(3, "jello", seed=71)
+    sc.groups[0].x[3, 1] = np.float32(np.nan)
+    with Simulation([sc]) as sim:
+        assert sim.step_status(1) == L.ERR_SIM
+        assert sim.device_errors() & L.DEVERR_NONFINITE
+
+
+def test_inverted_water_sets_det_error(gpu):
+    sc = blob_scene(3, "water", seed=72)
+    sc.groups[0].aux[5] = np.float32(-0.5)
+    with Simulation([sc]) as sim:
+        assert sim.step_status(1) == L.ERR_SIM
+        assert sim.device_errors() & L.DEVERR_DET
+
+
+def test_write_bgeo_roundtrip(gpu, tmp_path):
+    from test_bgeo import read_bgeo
+    sc = blob_scene(3, "jello", seed=80)
+    with Simulation([sc]) as sim:
+        sim.step(2)
+        p = str(tmp_path / "Frame000001.bgeo")
+        sim.write_bgeo(p, 0)
+        pos = sim.positions(0)
+    assert np.array_equal(read_bgeo(p), pos)
+
+
+# ------------------------------------------------ reference golden fixtures
+
+def _golden_files():
+    return sorted(glob.glob(os.path.join(GOLDEN, "ref3d_*.npz")))
+
+
+def golden_scene(z):
+    h, dt, n = float(z["h"]), float(z["dt"]), int(z["n_grid"])
+    groups = []
+    for gi in range(int(z["n_groups"])):
+        p = f"g{gi}_"
+        t = int(z[p + "type"])
+        if t == L.JELLO:
+            mat = S.jello(E=float(z[p + "E"]), nu=float(z[p + "nu"]), rho=float(z[p + "rho"]))
+        elif t == L.SNOW:
+            mat = S.snow(E=float(z[p + "E"]), nu=float(z[p + "nu"]), rho=float(z[p + "rho"]), theta_c=8e-2,
+                         theta_s=2e-2, xi=10.0)
+        else:
+            mat = S.water(K=2.51, rho=float(z[p + "rho"]), gamma=7.0)
+        from mpm_cuda_b200.sim import Group
+        groups.append(Group(material=mat, p_mass=float(z[p + "p_mass"]), p_vol=float(z[p + "p_vol"]),
+                            x=z[p + "in_x"], v=z[p + "in_v"], C=z[p + "in_C"], F=z[p + "in_F"],
+                            aux=z[p + "in_aux"]))
+    # the reference build's constants: 10h slip band, gravity -9.8 on y
+    return Scene(dim=3, n=(n, n, n), h=h, dt=dt, groups=groups, bc_type=L.BC_SLIP, bc_lo=11, bc_hi=10,
+                 gravity=(0.0, -9.8, 0.0), mass_eps=2.220446049250313e-16)
+
+
+@pytest.mark.parametrize("path", _golden_files(), ids=lambda p: os.path.basename(p))
+def test_matches_reference_build_golden(gpu, path):
+    z = np.load(path)
+    sc = golden_scene(z)
+    with Simulation([sc]) as sim:
+        done = 0
+        for k in (1, 10):
+            sim.step(k - done)
+            done = k
+            st = sim.get_state(0)
+            off = 0
+            for gi in range(int(z["n_groups"])):
+                n = z[f"g{gi}_in_x"].shape[0]
+                ref = {f: z[f"g{gi}_s{k}_{f}"] for f in ("x", "v", "C", "F", "aux")}
+                got = {f: st[f][off:off + n] for f in st}
+                tol = TOL_STEP if k == 1 else {"x": 5e-6, "v": 1e-3, "C": 1e-3, "F": 5e-5, "aux": 5e-5}
+                compare(got, ref, tol)
+                off += n
