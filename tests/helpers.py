@@ -12,6 +12,14 @@ from oracle import cpu as ocpu
 # field's largest magnitude (max |a - b| / max |b|), positions absolutely.
 TOL_STEP = {"x": 2e-6, "v": 1e-4, "C": 1e-4, "F": 1e-5, "aux": 1e-5}
 
+# Against the reference build's golden fixtures (tests/golden/ref3d_*.npz).
+# The reference computes stress and the snow SVD in FP32 with an
+# approximate-Jacobi SVD whose singular vectors are ill-conditioned for
+# near-equal singular values; the bound is max relative 1e-4 per substep.
+TOL_REF = {1: {"x": 1e-6, "v": 1e-4, "C": 1e-4, "F": 1e-4, "aux": 1e-4},
+           10: {"x": 5e-6, "v": 1e-3, "C": 1e-3, "F": 1e-3, "aux": 1e-3}}
+TOL_REF_MEDIAN = {1: 2e-6, 10: 2e-5}
+
 
 def group_from_arrays(mat: MaterialParams, h: float, ppc: int, x, v, C, F, aux) -> Group:
     d = x.shape[1]

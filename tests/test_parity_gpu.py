@@ -10,7 +10,7 @@ from mpm_cuda_b200 import _lib as L
 from mpm_cuda_b200 import scenes as S
 from mpm_cuda_b200.sim import Scene, Simulation
 
-from helpers import TOL_STEP, compare, group_from_arrays, oracle_for, rel_err
+from helpers import TOL_REF, TOL_STEP, compare, group_from_arrays, oracle_for, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -217,6 +217,5 @@ def test_matches_reference_build_golden(gpu, path):
                 n = z[f"g{gi}_in_x"].shape[0]
                 ref = {f: z[f"g{gi}_s{k}_{f}"] for f in ("x", "v", "C", "F", "aux")}
                 got = {f: st[f][off:off + n] for f in st}
-                tol = TOL_STEP if k == 1 else {"x": 5e-6, "v": 1e-3, "C": 1e-3, "F": 5e-5, "aux": 5e-5}
-                compare(got, ref, tol)
+                compare(got, ref, TOL_REF[k])
                 off += n
