@@ -49,10 +49,16 @@ enum mpm_boundary_type {
 
 /* P2G reduction modes */
 enum mpm_p2g_mode {
-    MPM_P2G_ATOMIC = 0,        /* shared-memory staged FP32 atomics (fast;
-                                  summation order varies run to run) */
-    MPM_P2G_DETERMINISTIC = 1  /* sorted gather reduction: bitwise identical
-                                  results across runs */
+    MPM_P2G_ATOMIC = 0,        /* particles binned by grid block; one fused
+                                  G2P + stress + P2G kernel per substep with
+                                  shared-memory grid tiles flushed by FP32
+                                  vector atomics (fast; summation order varies
+                                  run to run) */
+    MPM_P2G_DETERMINISTIC = 1, /* cell-sorted gather reduction: bitwise
+                                  identical results across runs */
+    MPM_P2G_DIRECT = 2         /* unbinned: one thread per particle, stencil
+                                  straight to global memory (the reference's
+                                  kernel structure; for comparison) */
 };
 
 /* Stress evaluation modes */
@@ -126,11 +132,13 @@ typedef struct mpm_scene_desc {
 } mpm_scene_desc;
 
 typedef struct mpm_options {
-    int p2g_mode;     /* enum mpm_p2g_mode */
-    int stress_mode;  /* enum mpm_stress_mode */
-    int use_graph;    /* capture the substep in a CUDA graph (default 1) */
-    int block_threads;/* threads per CTA for particle kernels; 0 = tuned */
-    int device;       /* CUDA device ordinal */
+    int p2g_mode;       /* enum mpm_p2g_mode */
+    int stress_mode;    /* enum mpm_stress_mode */
+    int use_graph;      /* capture the substep in a CUDA graph (default 1) */
+    int block_threads;  /* threads per CTA for the unbinned kernels; 0 = tuned */
+    int device;         /* CUDA device ordinal */
+    int rebin_interval; /* substeps between re-binnings of the particles
+                           (MPM_P2G_ATOMIC); 0 = tuned default */
 } mpm_options;
 
 typedef struct mpm_handle mpm_handle;
@@ -203,13 +211,22 @@ int mpm_set_p2g_mode(mpm_handle *h, int mode);
 int mpm_last_error(mpm_handle *h, char *buf, size_t cap);
 
 /* Per-stage device time of one substep, measured with CUDA events on the
- * handle's stream, averaged over n_substeps: out_ms[0..n_out) in stage order
- * (bin, p2g, grid_update, g2p).  Writes the stage names count to *n_written. */
+ * handle's stream and averaged over n_substeps (the handle advances by
+ * n_substeps).  out_ms[0..n_out) in stage order:
+ *   MPM_P2G_ATOMIC:  rebin (one re-binning), grid_update, g2p2g
+ *   MPM_P2G_DIRECT:  p2g, grid_update, g2p
+ *   MPM_P2G_DETERMINISTIC: g2p, sort, p2g_gather, grid_update
+ * *n_written receives the number of stages written. */
 int mpm_profile_stages(mpm_handle *h, int n_substeps, float *out_ms, int n_out,
                        int *n_written);
 
 /* Number of grid nodes with non-zero mass in one scene after the last step. */
 int mpm_count_active_nodes(mpm_handle *h, int scene, int64_t *n);
+
+/* Diagnostics of the binned path: *fallbacks counts particle gathers or
+ * scatters that left their block's shared-memory tile (served from global
+ * memory) since creation; *rebins counts re-binnings. */
+int mpm_get_bin_stats(mpm_handle *h, int64_t *fallbacks, int64_t *rebins);
 
 #ifdef __cplusplus
 }

@@ -18,7 +18,7 @@ LIB_PATH = os.path.join(HERE, "libmpm_b200.so")
 # enums (include/mpm_b200.h)
 JELLO, SNOW, WATER, SAND = 0, 1, 2, 3
 BC_STICKY, BC_SLIP, BC_SEPARATE = 0, 1, 2
-P2G_ATOMIC, P2G_DETERMINISTIC = 0, 1
+P2G_ATOMIC, P2G_DETERMINISTIC, P2G_DIRECT = 0, 1, 2
 STRESS_PLAIN, STRESS_SURROGATE = 0, 1
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_SIM, ERR_IO = 0, -1, -2, -3, -4, -5, -6
 DEVERR_OUT_OF_GRID, DEVERR_NONFINITE, DEVERR_DET, DEVERR_TIMEOUT = 1, 2, 4, 16
@@ -47,7 +47,7 @@ class SceneDesc(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("p2g_mode", C.c_int), ("stress_mode", C.c_int), ("use_graph", C.c_int),
-                ("block_threads", C.c_int), ("device", C.c_int)]
+                ("block_threads", C.c_int), ("device", C.c_int), ("rebin_interval", C.c_int)]
 
 
 EXPORTS = {
@@ -73,6 +73,7 @@ EXPORTS = {
     "mpm_last_error": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t]),
     "mpm_profile_stages": (C.c_int, [C.c_void_p, C.c_int, _FP, C.c_int, C.POINTER(C.c_int)]),
     "mpm_count_active_nodes": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]),
+    "mpm_get_bin_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
 }
 
 _lib = None

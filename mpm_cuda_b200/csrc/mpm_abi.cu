@@ -49,6 +49,7 @@ void mpm_default_options(mpm_options* opt) {
     opt->use_graph = 1;
     opt->block_threads = 0;
     opt->device = 0;
+    opt->rebin_interval = 0;
 }
 
 int mpm_create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options* opt,
@@ -130,7 +131,7 @@ int mpm_get_positions(mpm_handle* h, int scene, float* x, size_t cap) {
     size_t need = (size_t)h->eng.scene_count[scene] * h->eng.dim;
     if (cap < need)
         return fail(h, MPM_ERR_INVALID, "mpm_get_positions: cap %zu < %zu floats", cap, need);
-    return h->eng.get_state(scene, x, nullptr, nullptr, nullptr, nullptr);
+    return h->eng.get_positions(scene, x);
 }
 
 int mpm_get_state(mpm_handle* h, int scene, float* x, float* v, float* C, float* F, float* aux) {
@@ -162,6 +163,11 @@ int mpm_count_active_nodes(mpm_handle* h, int scene, int64_t* n) {
     return h->eng.count_active_nodes(scene, n);
 }
 
+int mpm_get_bin_stats(mpm_handle* h, int64_t* fallbacks, int64_t* rebins) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_get_bin_stats: NULL handle");
+    return h->eng.bin_stats(fallbacks, rebins);
+}
+
 int mpm_get_time(mpm_handle* h, double* t, int64_t* frame) {
     if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_get_time: NULL handle");
     if (t) *t = h->eng.current_time;
@@ -190,7 +196,7 @@ int mpm_write_bgeo_positions(const char* path, const float* x, int64_t n) {
 
 int mpm_set_p2g_mode(mpm_handle* h, int mode) {
     if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_set_p2g_mode: NULL handle");
-    if (mode != MPM_P2G_ATOMIC && mode != MPM_P2G_DETERMINISTIC)
+    if (mode != MPM_P2G_ATOMIC && mode != MPM_P2G_DETERMINISTIC && mode != MPM_P2G_DIRECT)
         return fail(h, MPM_ERR_INVALID, "mpm_set_p2g_mode: bad mode %d", mode);
     return h->eng.set_p2g_mode(mode);
 }

@@ -1,12 +1,15 @@
 // Engine implementation: validation, allocation, state I/O and the substep
-// launch sequence.
+// launch sequences (binned fused path, unbinned path).
 #include "mpm_engine.cuh"
+
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 
+#include "mpm_kernels_binned.cuh"
 #include "mpm_kernels_direct.cuh"
 
 namespace mpm {
@@ -14,6 +17,8 @@ namespace mpm {
 namespace {
 
 constexpr int kMaxGroups = 65535;
+constexpr int kDefaultRebinInterval = 16;
+enum { CNT_CHUNKS = 0, CNT_ACTIVE = 1, CNT_EPOCH = 2, CNT_CURSOR = 3, CNT_FALLBACK = 4, CNT_REBINS = 5, CNT_N = 8 };
 
 // out[id[i]] = in[i] for every plane (storage order -> creation order)
 __global__ void k_unpermute(const float* __restrict__ in, float* __restrict__ out, const uint32_t* __restrict__ id,
@@ -34,7 +39,17 @@ __global__ void k_permute_range(const float* __restrict__ in, float* __restrict_
     for (int p = 0; p < planes; ++p) out[p * cap + i] = in[p * cap + j];
 }
 
-unsigned grid_blocks(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+// positions of creation indices [lo, hi) as interleaved x[(id - lo) * dim + a]
+__global__ void k_gather_positions(const float* __restrict__ s, const uint32_t* __restrict__ id, long long n,
+                                   long long cap, int dim, long long lo, long long hi, float* __restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long j = id[i];
+    if (j < lo || j >= hi) return;
+    for (int a = 0; a < dim; ++a) out[(j - lo) * dim + a] = s[a * cap + i];
+}
+
+unsigned grid_blocks(long long n, int threads) { return (unsigned)std::max<long long>(1, (n + threads - 1) / threads); }
 
 }  // namespace
 
@@ -45,15 +60,23 @@ int Engine::cuda_fail(cudaError_t e, const char* what) {
     return e == cudaErrorMemoryAllocation ? MPM_ERR_NOMEM : MPM_ERR_CUDA;
 }
 
-#define MPM_CUDA_TRY(expr, what)                     \
-    do {                                             \
-        cudaError_t e_ = (expr);                     \
+#define MPM_CUDA_TRY(expr, what)                           \
+    do {                                                   \
+        cudaError_t e_ = (expr);                           \
         if (e_ != cudaSuccess) return cuda_fail(e_, what); \
     } while (0)
 
-int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options& o,
-                   std::string& msg) {
+int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options& o, std::string& msg) {
     opt = o;
+    if (opt.rebin_interval <= 0) opt.rebin_interval = kDefaultRebinInterval;
+    if (opt.p2g_mode < MPM_P2G_ATOMIC || opt.p2g_mode > MPM_P2G_DIRECT) {
+        msg = "mpm_create: bad p2g_mode";
+        return MPM_ERR_INVALID;
+    }
+    if (opt.stress_mode != MPM_STRESS_PLAIN) {
+        msg = "mpm_create: the surrogate stress needs a trained model (mpm_surrogate_load)";
+        return MPM_ERR_UNSUPPORTED;
+    }
     char buf[512];
     auto bad = [&](int code, const char* text) {
         msg = text;
@@ -78,8 +101,7 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
         }
         if (d.bc_type < MPM_BC_STICKY || d.bc_type > MPM_BC_SEPARATE || d.bc_lo < 0 || d.bc_hi < 0)
             return bad(MPM_ERR_INVALID, "mpm_create: bad boundary descriptor");
-        if (d.n_groups < 0 || (d.n_groups > 0 && !d.groups))
-            return bad(MPM_ERR_INVALID, "mpm_create: bad group list");
+        if (d.n_groups < 0 || (d.n_groups > 0 && !d.groups)) return bad(MPM_ERR_INVALID, "mpm_create: bad group list");
         for (int gi = 0; gi < d.n_groups; ++gi) {
             const mpm_group_desc& g = d.groups[gi];
             const mpm_material_desc& m = g.material;
@@ -87,8 +109,7 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
                 msg = "mpm_create: SAND is declared by the reference but not implemented";
                 return MPM_ERR_UNSUPPORTED;
             }
-            if (m.type < MPM_JELLO || m.type > MPM_WATER)
-                return bad(MPM_ERR_INVALID, "mpm_create: unknown material type");
+            if (m.type < MPM_JELLO || m.type > MPM_WATER) return bad(MPM_ERR_INVALID, "mpm_create: unknown material type");
             // Elasiticity.cuh:34-41 range checks
             if (m.E < 0.0) return bad(MPM_ERR_INVALID, "mpm_create: Youngs Modulus is out of range");
             if (m.nu < 0.0 || m.nu >= 0.5) return bad(MPM_ERR_INVALID, "mpm_create: Poisson ratio is out of range");
@@ -110,8 +131,7 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     scene_begin.assign(n_scenes, 0);
     scene_count.assign(n_scenes, 0);
     long long block_off = 0, p_off = 0;
-    constexpr int side3 = 4, side2 = 8;
-    const int side = dim == 3 ? side3 : side2;
+    const int side = dim == 3 ? 4 : 8;
     for (int s = 0; s < n_scenes; ++s) {
         const mpm_scene_desc& d = scenes[s];
         SceneParams sp{};
@@ -142,8 +162,8 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
             GroupParams gp{};
             gp.scene = s;
             gp.type = m.type;
-            double mu = m.E / (2.0 * (1.0 + m.nu));
-            double la = m.E * m.nu / ((1.0 + m.nu) * (1.0 - 2.0 * m.nu));
+            const double mu = m.E / (2.0 * (1.0 + m.nu));
+            const double la = m.E * m.nu / ((1.0 + m.nu) * (1.0 - 2.0 * m.nu));
             gp.mu = (float)mu;
             gp.lambda = (float)la;
             gp.xi = (float)m.xi;
@@ -158,6 +178,7 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
         }
         scene_count[s] = p_off - scene_begin[s];
     }
+    if (block_off > 0x7fffffffLL) return bad(MPM_ERR_INVALID, "mpm_create: grids too large");
     total_blocks = block_off;
     current_time = 0.0;
     current_frame = 0;
@@ -184,8 +205,7 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
                     }
                     for (int e = 0; e < D * D; ++e) {
                         host[(size_t)(PC + e) * cap + i] = g.C ? g.C[k * D * D + e] : 0.f;
-                        host[(size_t)(PF + e) * cap + i] =
-                            g.F ? g.F[k * D * D + e] : ((e % (D + 1) == 0) ? 1.f : 0.f);
+                        host[(size_t)(PF + e) * cap + i] = g.F ? g.F[k * D * D + e] : ((e % (D + 1) == 0) ? 1.f : 0.f);
                     }
                     host[(size_t)PA * cap + i] = g.aux ? g.aux[k] : 1.f;
                     grp_h[i] = (uint16_t)gidx;
@@ -202,8 +222,9 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
         msg = std::string("mpm_create: cudaSetDevice: ") + cudaGetErrorString(e);
         return MPM_ERR_CUDA;
     }
+    cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device);
     auto alloc = [&](void** p, size_t bytes, const char* what) -> int {
-        cudaError_t ae = cudaMalloc(p, bytes);
+        cudaError_t ae = cudaMalloc(p, std::max<size_t>(bytes, 16));
         if (ae != cudaSuccess) {
             msg = std::string("mpm_create: cudaMalloc ") + what + ": " + cudaGetErrorString(ae);
             return ae == cudaErrorMemoryAllocation ? MPM_ERR_NOMEM : MPM_ERR_CUDA;
@@ -212,12 +233,11 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     };
     int rc;
     const size_t state_bytes = (size_t)n_planes * cap * sizeof(float);
-    if ((rc = alloc((void**)&state, state_bytes, "state")) != MPM_OK) return rc;
-    if ((rc = alloc((void**)&state_alt, state_bytes, "state_alt")) != MPM_OK) return rc;
-    if ((rc = alloc((void**)&grp, cap * sizeof(uint16_t), "grp")) != MPM_OK) return rc;
-    if ((rc = alloc((void**)&grp_alt, cap * sizeof(uint16_t), "grp_alt")) != MPM_OK) return rc;
-    if ((rc = alloc((void**)&id, cap * sizeof(uint32_t), "id")) != MPM_OK) return rc;
-    if ((rc = alloc((void**)&id_alt, cap * sizeof(uint32_t), "id_alt")) != MPM_OK) return rc;
+    for (int p = 0; p < 2; ++p) {
+        if ((rc = alloc((void**)&st[p], state_bytes, "state")) != MPM_OK) return rc;
+        if ((rc = alloc((void**)&gp[p], cap * sizeof(uint16_t), "grp")) != MPM_OK) return rc;
+        if ((rc = alloc((void**)&ids[p], cap * sizeof(uint32_t), "id")) != MPM_OK) return rc;
+    }
     if ((rc = alloc((void**)&groups_d, std::max<size_t>(1, groups_h.size()) * sizeof(GroupParams), "groups")) != MPM_OK)
         return rc;
     if ((rc = alloc((void**)&scenes_d, scenes_h.size() * sizeof(SceneParams), "scenes")) != MPM_OK) return rc;
@@ -225,14 +245,28 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     if ((rc = alloc((void**)&grid_mom, grid_bytes, "grid_mom")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&grid_vel, grid_bytes, "grid_vel")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&err_d, sizeof(unsigned), "err")) != MPM_OK) return rc;
+    if ((rc = alloc((void**)&key, cap * sizeof(int), "key")) != MPM_OK) return rc;
+    if ((rc = alloc((void**)&rank, cap * sizeof(int), "rank")) != MPM_OK) return rc;
+    if ((rc = alloc((void**)&blk_count, total_blocks * sizeof(int), "blk_count")) != MPM_OK) return rc;
+    if ((rc = alloc((void**)&blk_start, total_blocks * sizeof(int), "blk_start")) != MPM_OK) return rc;
+    if ((rc = alloc((void**)&blk_flag, total_blocks * sizeof(unsigned), "blk_flag")) != MPM_OK) return rc;
+    if ((rc = alloc((void**)&active, total_blocks * sizeof(int), "active")) != MPM_OK) return rc;
+    if ((rc = alloc((void**)&blk_epoch, total_blocks * sizeof(int), "blk_epoch")) != MPM_OK) return rc;
+    if ((rc = alloc((void**)&counters, CNT_N * sizeof(int), "counters")) != MPM_OK) return rc;
+    max_chunks = cap / kChunk + std::min<long long>(cap, total_blocks) + 1;
+    if ((rc = alloc((void**)&chunks, max_chunks * sizeof(Chunk), "chunks")) != MPM_OK) return rc;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp_bytes, blk_count, blk_start, (int)total_blocks);
+    if ((rc = alloc(&scan_tmp, scan_tmp_bytes, "scan temp")) != MPM_OK) return rc;
+    if ((rc = alloc((void**)&pos_out, cap * D * sizeof(float), "positions")) != MPM_OK) return rc;
+
     e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         msg = std::string("mpm_create: stream: ") + cudaGetErrorString(e);
         return MPM_ERR_CUDA;
     }
-    e = cudaMemcpy(state, host.data(), state_bytes, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(grp, grp_h.data(), cap * sizeof(uint16_t), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(id, id_h.data(), cap * sizeof(uint32_t), cudaMemcpyHostToDevice);
+    e = cudaMemcpy(st[0], host.data(), state_bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(gp[0], grp_h.data(), cap * sizeof(uint16_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(ids[0], id_h.data(), cap * sizeof(uint32_t), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !groups_h.empty())
         e = cudaMemcpy(groups_d, groups_h.data(), groups_h.size() * sizeof(GroupParams), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
@@ -240,89 +274,195 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     if (e == cudaSuccess) e = cudaMemset(grid_mom, 0, grid_bytes);
     if (e == cudaSuccess) e = cudaMemset(grid_vel, 0, grid_bytes);
     if (e == cudaSuccess) e = cudaMemset(err_d, 0, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(blk_flag, 0, total_blocks * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(blk_epoch, 0xff, total_blocks * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(counters, 0, CNT_N * sizeof(int));
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         msg = std::string("mpm_create: upload: ") + cudaGetErrorString(e);
         return MPM_ERR_CUDA;
     }
-    graph_dirty = true;
+    int per_sm = 0;
+    if (dim == 3)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_g2p2g<3>, kChunk, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_g2p2g<2>, kChunk, 0);
+    fused_ctas = num_sms * std::max(1, per_sm);
+    update_ctas = (int)std::min<long long>((total_blocks + 3) / 4, (long long)num_sms * 8);
+    cur = 0;
+    grid_dirty = true;
     return MPM_OK;
 }
 
 void Engine::release() {
     if (device >= 0) cudaSetDevice(device);
-    drop_graph();
+    drop_graphs();
     if (stream) cudaStreamSynchronize(stream);
-    cudaFree(state);
-    cudaFree(state_alt);
-    cudaFree(grp);
-    cudaFree(grp_alt);
-    cudaFree(id);
-    cudaFree(id_alt);
-    cudaFree(groups_d);
-    cudaFree(scenes_d);
-    cudaFree(grid_mom);
-    cudaFree(grid_vel);
-    cudaFree(err_d);
-    if (stream) cudaStreamDestroy(stream);
-    state = state_alt = nullptr;
-    grp = grp_alt = nullptr;
-    id = id_alt = nullptr;
+    for (int p = 0; p < 2; ++p) {
+        cudaFree(st[p]);
+        cudaFree(gp[p]);
+        cudaFree(ids[p]);
+        st[p] = nullptr;
+        gp[p] = nullptr;
+        ids[p] = nullptr;
+    }
+    void* ptrs[] = {groups_d, scenes_d, grid_mom, grid_vel, err_d, key, rank, blk_count, blk_start,
+                    blk_flag, active, blk_epoch, counters, chunks, scan_tmp, pos_out};
+    for (void* p : ptrs) cudaFree(p);
     groups_d = nullptr;
     scenes_d = nullptr;
     grid_mom = grid_vel = nullptr;
     err_d = nullptr;
+    key = rank = blk_count = blk_start = nullptr;
+    blk_flag = nullptr;
+    active = blk_epoch = counters = nullptr;
+    chunks = nullptr;
+    scan_tmp = nullptr;
+    pos_out = nullptr;
+    if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
 }
 
-void Engine::drop_graph() {
-    if (graph_exec) cudaGraphExecDestroy(graph_exec);
-    graph_exec = nullptr;
-    graph_dirty = true;
+void Engine::drop_graphs() {
+    for (auto& row : graphs)
+        for (auto& g : row) {
+            if (g) cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
 }
 
-void Engine::enqueue_substep() {
-    ParticleBuf pb{state, cap, grp, id};
+// ---------------------------------------------------------- launches --
+
+void Engine::enqueue_direct_substep() {
+    const ParticleBuf pb = buf(cur);
     const int n_scenes = (int)scenes_h.size();
     const long long nodes = total_blocks * 64;
+    const int bt = opt.block_threads > 0 ? opt.block_threads : 128;
     if (dim == 3) {
         if (n_particles > 0)
-            k_p2g_direct<3><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
-                                                                               grid_mom, err_d);
+            k_p2g_direct<3><<<grid_blocks(n_particles, bt), bt, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
+                                                                             grid_mom, err_d);
         k_grid_update_dense<3><<<grid_blocks(nodes, 256), 256, 0, stream>>>(grid_mom, grid_vel, total_blocks,
                                                                             scenes_d, n_scenes, 1);
         if (n_particles > 0)
-            k_g2p_direct<3><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
-                                                                               grid_vel, err_d);
+            k_g2p_direct<3><<<grid_blocks(n_particles, bt), bt, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
+                                                                             grid_vel, err_d);
     } else {
         if (n_particles > 0)
-            k_p2g_direct<2><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
-                                                                               grid_mom, err_d);
+            k_p2g_direct<2><<<grid_blocks(n_particles, bt), bt, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
+                                                                             grid_mom, err_d);
         k_grid_update_dense<2><<<grid_blocks(nodes, 256), 256, 0, stream>>>(grid_mom, grid_vel, total_blocks,
                                                                             scenes_d, n_scenes, 1);
         if (n_particles > 0)
-            k_g2p_direct<2><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
-                                                                               grid_vel, err_d);
+            k_g2p_direct<2><<<grid_blocks(n_particles, bt), bt, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
+                                                                             grid_vel, err_d);
     }
 }
 
-int Engine::build_graph() {
-    drop_graph();
+// counting sort of the particles of buffer `from` by home block into the
+// other buffer, and the chunk table of the result
+void Engine::enqueue_rebin(int from) {
+    const int to = 1 - from;
+    cudaMemsetAsync(blk_count, 0, total_blocks * sizeof(int), stream);
+    cudaMemsetAsync(counters + CNT_CHUNKS, 0, sizeof(int), stream);
+    if (n_particles > 0) {
+        if (dim == 3)
+            k_bin_count<3><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), n_particles, groups_d,
+                                                                              scenes_d, key, rank, blk_count);
+        else
+            k_bin_count<2><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), n_particles, groups_d,
+                                                                              scenes_d, key, rank, blk_count);
+    }
+    cub::DeviceScan::ExclusiveSum(scan_tmp, scan_tmp_bytes, blk_count, blk_start, (int)total_blocks, stream);
+    if (n_particles > 0) {
+        if (dim == 3)
+            k_bin_scatter<3><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), buf(to), n_particles, key,
+                                                                                rank, blk_start);
+        else
+            k_bin_scatter<2><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), buf(to), n_particles, key,
+                                                                                rank, blk_start);
+    }
+    k_make_chunks<<<grid_blocks(total_blocks, 256), 256, 0, stream>>>(blk_count, blk_start, total_blocks, chunks,
+                                                                      counters + CNT_CHUNKS);
+    k_count_rebin<<<1, 1, 0, stream>>>(counters + CNT_REBINS);
+}
+
+void Engine::enqueue_fused_substep(int parity) {
+    const int n_scenes = (int)scenes_h.size();
+    if (dim == 3)
+        k_grid_update_active<3><<<update_ctas, 256, 0, stream>>>(grid_mom, grid_vel, active, counters + CNT_ACTIVE,
+                                                                 blk_flag, blk_epoch, counters + CNT_EPOCH, scenes_d,
+                                                                 n_scenes);
+    else
+        k_grid_update_active<2><<<update_ctas, 256, 0, stream>>>(grid_mom, grid_vel, active, counters + CNT_ACTIVE,
+                                                                 blk_flag, blk_epoch, counters + CNT_EPOCH, scenes_d,
+                                                                 n_scenes);
+    cudaMemsetAsync(counters + CNT_ACTIVE, 0, sizeof(int), stream);
+    cudaMemsetAsync(counters + CNT_CURSOR, 0, sizeof(int), stream);
+    FusedArgs A;
+    A.chunks = chunks;
+    A.n_chunks = counters + CNT_CHUNKS;
+    A.cursor = counters + CNT_CURSOR;
+    A.groups = groups_d;
+    A.scenes = scenes_d;
+    A.n_scenes = n_scenes;
+    A.grid_vel = grid_vel;
+    A.grid_mom = grid_mom;
+    A.blk_flag = blk_flag;
+    A.active = active;
+    A.n_active = counters + CNT_ACTIVE;
+    A.epoch = counters + CNT_EPOCH;
+    A.err_word = err_d;
+    A.fallback = (unsigned*)(counters + CNT_FALLBACK);
+    if (dim == 3)
+        k_g2p2g<3><<<fused_ctas, kChunk, 0, stream>>>(buf(parity), A);
+    else
+        k_g2p2g<2><<<fused_ctas, kChunk, 0, stream>>>(buf(parity), A);
+}
+
+// makes grid_mom hold the P2G of the current state (binned path): sorts the
+// particles into fresh chunks and scatters them straight to global memory
+int Engine::prologue() {
+    const size_t grid_bytes = (size_t)total_blocks * 64 * sizeof(float4);
+    MPM_CUDA_TRY(cudaMemsetAsync(grid_mom, 0, grid_bytes, stream), "prologue clear");
+    MPM_CUDA_TRY(cudaMemsetAsync(blk_flag, 0, total_blocks * sizeof(unsigned), stream), "prologue flags");
+    MPM_CUDA_TRY(cudaMemsetAsync(counters + CNT_ACTIVE, 0, sizeof(int), stream), "prologue counters");
+    enqueue_rebin(cur);
+    cur = 1 - cur;
+    steps_since_rebin = 0;
+    if (n_particles > 0) {
+        if (dim == 3)
+            k_p2g_prologue<3><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(
+                buf(cur), n_particles, groups_d, scenes_d, grid_mom, blk_flag, active, counters + CNT_ACTIVE, err_d);
+        else
+            k_p2g_prologue<2><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(
+                buf(cur), n_particles, groups_d, scenes_d, grid_mom, blk_flag, active, counters + CNT_ACTIVE, err_d);
+    }
+    MPM_CUDA_TRY(cudaGetLastError(), "prologue launch");
+    grid_dirty = false;
+    return MPM_OK;
+}
+
+int Engine::build_graph(int parity, int rebin) {
     cudaGraph_t g = nullptr;
     MPM_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "graph capture begin");
-    enqueue_substep();
+    if (rebin) {
+        enqueue_rebin(parity);
+        enqueue_fused_substep(1 - parity);
+    } else {
+        enqueue_fused_substep(parity);
+    }
     cudaError_t e = cudaStreamEndCapture(stream, &g);
     if (e != cudaSuccess) {
         if (g) cudaGraphDestroy(g);
         return cuda_fail(e, "graph capture end");
     }
-    e = cudaGraphInstantiate(&graph_exec, g, 0);
+    e = cudaGraphInstantiate(&graphs[parity][rebin], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
-        graph_exec = nullptr;
+        graphs[parity][rebin] = nullptr;
         return cuda_fail(e, "graph instantiate");
     }
-    graph_dirty = false;
     return MPM_OK;
 }
 
@@ -332,20 +472,59 @@ int Engine::step(int n) {
         return MPM_ERR_INVALID;
     }
     MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
-    if (opt.use_graph) {
-        if (graph_dirty || !graph_exec) {
-            int rc = build_graph();
+    if (!fused()) {
+        if (grid_dirty) {
+            MPM_CUDA_TRY(cudaMemsetAsync(grid_mom, 0, (size_t)total_blocks * 64 * sizeof(float4), stream),
+                         "grid clear");
+            grid_dirty = false;
+        }
+        if (opt.use_graph) {
+            if (!graphs[cur][0]) {
+                cudaGraph_t g = nullptr;
+                MPM_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture begin");
+                enqueue_direct_substep();
+                cudaError_t e = cudaStreamEndCapture(stream, &g);
+                if (e != cudaSuccess) return cuda_fail(e, "capture end");
+                e = cudaGraphInstantiate(&graphs[cur][0], g, 0);
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
+            }
+            for (int i = 0; i < n; ++i) MPM_CUDA_TRY(cudaGraphLaunch(graphs[cur][0], stream), "graph launch");
+        } else {
+            for (int i = 0; i < n; ++i) enqueue_direct_substep();
+            MPM_CUDA_TRY(cudaGetLastError(), "kernel launch");
+        }
+    } else {
+        if (grid_dirty) {
+            int rc = prologue();
             if (rc != MPM_OK) return rc;
         }
-        for (int i = 0; i < n; ++i) MPM_CUDA_TRY(cudaGraphLaunch(graph_exec, stream), "graph launch");
-    } else {
-        for (int i = 0; i < n; ++i) enqueue_substep();
-        MPM_CUDA_TRY(cudaGetLastError(), "kernel launch");
+        for (int i = 0; i < n; ++i) {
+            const int rebin = steps_since_rebin >= opt.rebin_interval ? 1 : 0;
+            if (opt.use_graph) {
+                if (!graphs[cur][rebin]) {
+                    int rc = build_graph(cur, rebin);
+                    if (rc != MPM_OK) return rc;
+                }
+                MPM_CUDA_TRY(cudaGraphLaunch(graphs[cur][rebin], stream), "graph launch");
+            } else {
+                if (rebin) enqueue_rebin(cur);
+                enqueue_fused_substep(rebin ? 1 - cur : cur);
+                MPM_CUDA_TRY(cudaGetLastError(), "kernel launch");
+            }
+            if (rebin) {
+                cur = 1 - cur;
+                steps_since_rebin = 0;
+            }
+            ++steps_since_rebin;
+        }
     }
     current_frame += n;
     current_time += (double)n * (scenes_h.empty() ? 0.0 : (double)scenes_h[0].dt);
     return MPM_OK;
 }
+
+// ----------------------------------------------------------- queries --
 
 int Engine::read_errors(uint32_t* bits) {
     unsigned v = 0;
@@ -367,10 +546,9 @@ int Engine::sync_and_check() {
     int rc = read_errors(&bits);
     if (rc != MPM_OK) return rc;
     if (bits) {
-        char buf[256];
-        std::snprintf(buf, sizeof(buf), "device error word 0x%x (1 out of grid, 2 non-finite, 4 det<=0, 16 timeout)",
-                      bits);
-        last_error = buf;
+        char b[256];
+        std::snprintf(b, sizeof(b), "device error word 0x%x (1 out of grid, 2 non-finite, 4 det<=0, 16 timeout)", bits);
+        last_error = b;
         return MPM_ERR_SIM;
     }
     return MPM_OK;
@@ -378,8 +556,22 @@ int Engine::sync_and_check() {
 
 int Engine::unpermute_to_alt() {
     if (n_particles == 0) return MPM_OK;
-    k_unpermute<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(state, state_alt, id, n_particles, cap, n_planes);
+    k_unpermute<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(st[cur], st[1 - cur], ids[cur], n_particles, cap,
+                                                                   n_planes);
     MPM_CUDA_TRY(cudaGetLastError(), "unpermute launch");
+    return MPM_OK;
+}
+
+int Engine::get_positions(int scene, float* out) {
+    MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    const long long b = scene_begin[scene], n = scene_count[scene];
+    if (n == 0) return MPM_OK;
+    k_gather_positions<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(st[cur], ids[cur], n_particles, cap, dim, b,
+                                                                          b + n, pos_out);
+    MPM_CUDA_TRY(cudaGetLastError(), "gather launch");
+    MPM_CUDA_TRY(cudaMemcpyAsync(out, pos_out, (size_t)n * dim * sizeof(float), cudaMemcpyDeviceToHost, stream),
+                 "positions download");
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
     return MPM_OK;
 }
 
@@ -391,13 +583,8 @@ int Engine::get_state(int scene, float* x, float* v, float* C, float* F, float* 
     const long long b = scene_begin[scene], n = scene_count[scene];
     if (n == 0) return MPM_OK;
     const int D = dim;
+    const float* alt = st[1 - cur];
     std::vector<float> plane(n);
-    auto fetch = [&](int p) -> int {
-        MPM_CUDA_TRY(cudaMemcpy(plane.data(), state_alt + (size_t)p * cap + b, n * sizeof(float),
-                                cudaMemcpyDeviceToHost),
-                     "state download");
-        return MPM_OK;
-    };
     struct Field {
         float* dst;
         int first, count;
@@ -405,15 +592,16 @@ int Engine::get_state(int scene, float* x, float* v, float* C, float* F, float* 
     for (auto& f : fields) {
         if (!f.dst) continue;
         for (int c = 0; c < f.count; ++c) {
-            if ((rc = fetch(f.first + c)) != MPM_OK) return rc;
+            MPM_CUDA_TRY(cudaMemcpy(plane.data(), alt + (size_t)(f.first + c) * cap + b, n * sizeof(float),
+                                    cudaMemcpyDeviceToHost),
+                         "state download");
             for (long long i = 0; i < n; ++i) f.dst[i * f.count + c] = plane[i];
         }
     }
     return MPM_OK;
 }
 
-int Engine::set_state(int scene, const float* x, const float* v, const float* C, const float* F,
-                      const float* aux) {
+int Engine::set_state(int scene, const float* x, const float* v, const float* C, const float* F, const float* aux) {
     MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
     int rc = unpermute_to_alt();
     if (rc != MPM_OK) return rc;
@@ -421,6 +609,7 @@ int Engine::set_state(int scene, const float* x, const float* v, const float* C,
     const long long b = scene_begin[scene], n = scene_count[scene];
     if (n == 0) return MPM_OK;
     const int D = dim;
+    float* alt = st[1 - cur];
     std::vector<float> plane(n);
     struct Field {
         const float* src;
@@ -430,15 +619,16 @@ int Engine::set_state(int scene, const float* x, const float* v, const float* C,
         if (!f.src) continue;
         for (int c = 0; c < f.count; ++c) {
             for (long long i = 0; i < n; ++i) plane[i] = f.src[i * f.count + c];
-            MPM_CUDA_TRY(cudaMemcpy(state_alt + (size_t)(f.first + c) * cap + b, plane.data(), n * sizeof(float),
+            MPM_CUDA_TRY(cudaMemcpy(alt + (size_t)(f.first + c) * cap + b, plane.data(), n * sizeof(float),
                                     cudaMemcpyHostToDevice),
                          "state upload");
         }
     }
-    k_permute_range<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(state_alt, state, id, n_particles, cap,
+    k_permute_range<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(alt, st[cur], ids[cur], n_particles, cap,
                                                                        n_planes, b, b + n);
     MPM_CUDA_TRY(cudaGetLastError(), "permute launch");
     MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
+    grid_dirty = true;
     return MPM_OK;
 }
 
@@ -449,6 +639,18 @@ int Engine::get_grid(int scene, float* mass, float* vel) {
     std::vector<float4> blk((size_t)sc.n_nodes);
     MPM_CUDA_TRY(cudaMemcpy(blk.data(), grid_vel + sc.node_off, sc.n_nodes * sizeof(float4), cudaMemcpyDeviceToHost),
                  "grid download");
+    if (fused()) {
+        // blocks not stamped by the last grid update hold stale values
+        std::vector<int> ep((size_t)sc.n_blocks);
+        int cnt[CNT_N];
+        MPM_CUDA_TRY(cudaMemcpy(ep.data(), blk_epoch + sc.block_off, sc.n_blocks * sizeof(int), cudaMemcpyDeviceToHost),
+                     "epoch download");
+        MPM_CUDA_TRY(cudaMemcpy(cnt, counters, sizeof(cnt), cudaMemcpyDeviceToHost), "counter download");
+        const int last = cnt[CNT_EPOCH] - 1;
+        for (long long b = 0; b < sc.n_blocks; ++b)
+            if (ep[b] != last)
+                for (int k = 0; k < 64; ++k) blk[b * 64 + k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     const int side = dim == 3 ? 4 : 8;
     const int D = dim;
     for (int iz = 0; iz < sc.n[2]; ++iz)
@@ -479,53 +681,127 @@ int Engine::count_active_nodes(int scene, int64_t* n) {
     return MPM_OK;
 }
 
+int Engine::bin_stats(int64_t* fallbacks, int64_t* rebins) {
+    MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
+    int cnt[CNT_N];
+    MPM_CUDA_TRY(cudaMemcpy(cnt, counters, sizeof(cnt), cudaMemcpyDeviceToHost), "counter download");
+    if (fallbacks) *fallbacks = (int64_t)(unsigned)cnt[CNT_FALLBACK];
+    if (rebins) *rebins = cnt[CNT_REBINS];
+    return MPM_OK;
+}
+
 int Engine::set_p2g_mode(int mode) {
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
     opt.p2g_mode = mode;
-    drop_graph();
+    drop_graphs();
+    grid_dirty = true;
     return MPM_OK;
 }
 
 int Engine::profile_stages(int n, float* out_ms, int n_out, int* n_written) {
     MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
-    ParticleBuf pb{state, cap, grp, id};
+    cudaEvent_t ev[4];
+    for (auto& e : ev) cudaEventCreate(&e);
+    float acc[3] = {0.f, 0.f, 0.f};
     const int n_scenes = (int)scenes_h.size();
     const long long nodes = total_blocks * 64;
-    const int n_stages = 3;
-    cudaEvent_t ev[n_stages + 1];
-    for (auto& e : ev) cudaEventCreate(&e);
-    float acc[n_stages] = {0.f, 0.f, 0.f};
-    for (int it = 0; it < n; ++it) {
-        cudaEventRecord(ev[0], stream);
-        if (dim == 3) {
-            k_p2g_direct<3><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
-                                                                               grid_mom, err_d);
-            cudaEventRecord(ev[1], stream);
-            k_grid_update_dense<3><<<grid_blocks(nodes, 256), 256, 0, stream>>>(grid_mom, grid_vel, total_blocks,
-                                                                                scenes_d, n_scenes, 1);
-            cudaEventRecord(ev[2], stream);
-            k_g2p_direct<3><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
-                                                                               grid_vel, err_d);
-        } else {
-            k_p2g_direct<2><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
-                                                                               grid_mom, err_d);
-            cudaEventRecord(ev[1], stream);
-            k_grid_update_dense<2><<<grid_blocks(nodes, 256), 256, 0, stream>>>(grid_mom, grid_vel, total_blocks,
-                                                                                scenes_d, n_scenes, 1);
-            cudaEventRecord(ev[2], stream);
-            k_g2p_direct<2><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
-                                                                               grid_vel, err_d);
+    const int bt = opt.block_threads > 0 ? opt.block_threads : 128;
+    if (fused()) {
+        if (grid_dirty) {
+            int rc = prologue();
+            if (rc != MPM_OK) return rc;
         }
-        cudaEventRecord(ev[3], stream);
-        cudaEventSynchronize(ev[3]);
-        for (int s = 0; s < n_stages; ++s) {
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, ev[s], ev[s + 1]);
-            acc[s] += ms;
+        // one re-binning
+        cudaEventRecord(ev[0], stream);
+        enqueue_rebin(cur);
+        cudaEventRecord(ev[1], stream);
+        cudaEventSynchronize(ev[1]);
+        cudaEventElapsedTime(&acc[0], ev[0], ev[1]);
+        cur = 1 - cur;
+        steps_since_rebin = 0;
+        acc[0] *= n;
+        for (int it = 0; it < n; ++it) {
+            cudaEventRecord(ev[0], stream);
+            if (dim == 3)
+                k_grid_update_active<3><<<update_ctas, 256, 0, stream>>>(grid_mom, grid_vel, active,
+                                                                         counters + CNT_ACTIVE, blk_flag, blk_epoch,
+                                                                         counters + CNT_EPOCH, scenes_d, n_scenes);
+            else
+                k_grid_update_active<2><<<update_ctas, 256, 0, stream>>>(grid_mom, grid_vel, active,
+                                                                         counters + CNT_ACTIVE, blk_flag, blk_epoch,
+                                                                         counters + CNT_EPOCH, scenes_d, n_scenes);
+            cudaEventRecord(ev[1], stream);
+            cudaMemsetAsync(counters + CNT_ACTIVE, 0, sizeof(int), stream);
+            cudaMemsetAsync(counters + CNT_CURSOR, 0, sizeof(int), stream);
+            cudaEventRecord(ev[2], stream);
+            FusedArgs A;
+            A.chunks = chunks;
+            A.n_chunks = counters + CNT_CHUNKS;
+            A.cursor = counters + CNT_CURSOR;
+            A.groups = groups_d;
+            A.scenes = scenes_d;
+            A.n_scenes = n_scenes;
+            A.grid_vel = grid_vel;
+            A.grid_mom = grid_mom;
+            A.blk_flag = blk_flag;
+            A.active = active;
+            A.n_active = counters + CNT_ACTIVE;
+            A.epoch = counters + CNT_EPOCH;
+            A.err_word = err_d;
+            A.fallback = (unsigned*)(counters + CNT_FALLBACK);
+            if (dim == 3)
+                k_g2p2g<3><<<fused_ctas, kChunk, 0, stream>>>(buf(cur), A);
+            else
+                k_g2p2g<2><<<fused_ctas, kChunk, 0, stream>>>(buf(cur), A);
+            cudaEventRecord(ev[3], stream);
+            cudaEventSynchronize(ev[3]);
+            float a = 0.f, b = 0.f;
+            cudaEventElapsedTime(&a, ev[0], ev[1]);
+            cudaEventElapsedTime(&b, ev[2], ev[3]);
+            acc[1] += a;
+            acc[2] += b;
+            ++steps_since_rebin;
+        }
+    } else {
+        const ParticleBuf pb = buf(cur);
+        if (grid_dirty) {
+            cudaMemsetAsync(grid_mom, 0, (size_t)total_blocks * 64 * sizeof(float4), stream);
+            grid_dirty = false;
+        }
+        for (int it = 0; it < n; ++it) {
+            cudaEventRecord(ev[0], stream);
+            if (dim == 3) {
+                k_p2g_direct<3><<<grid_blocks(n_particles, bt), bt, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
+                                                                                 grid_mom, err_d);
+                cudaEventRecord(ev[1], stream);
+                k_grid_update_dense<3><<<grid_blocks(nodes, 256), 256, 0, stream>>>(grid_mom, grid_vel, total_blocks,
+                                                                                    scenes_d, n_scenes, 1);
+                cudaEventRecord(ev[2], stream);
+                k_g2p_direct<3><<<grid_blocks(n_particles, bt), bt, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
+                                                                                 grid_vel, err_d);
+            } else {
+                k_p2g_direct<2><<<grid_blocks(n_particles, bt), bt, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
+                                                                                 grid_mom, err_d);
+                cudaEventRecord(ev[1], stream);
+                k_grid_update_dense<2><<<grid_blocks(nodes, 256), 256, 0, stream>>>(grid_mom, grid_vel, total_blocks,
+                                                                                    scenes_d, n_scenes, 1);
+                cudaEventRecord(ev[2], stream);
+                k_g2p_direct<2><<<grid_blocks(n_particles, bt), bt, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
+                                                                                 grid_vel, err_d);
+            }
+            cudaEventRecord(ev[3], stream);
+            cudaEventSynchronize(ev[3]);
+            for (int s = 0; s < 3; ++s) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ev[s], ev[s + 1]);
+                acc[s] += ms;
+            }
         }
     }
     for (auto& e : ev) cudaEventDestroy(e);
     MPM_CUDA_TRY(cudaGetLastError(), "profile launch");
-    int w = std::min(n_out, n_stages);
+    const int w = std::min(n_out, 3);
     for (int s = 0; s < w; ++s) out_ms[s] = acc[s] / n;
     if (n_written) *n_written = w;
     current_frame += n;

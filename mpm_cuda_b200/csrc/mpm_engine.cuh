@@ -1,4 +1,4 @@
-// Engine behind the C-ABI handle: device memory, stream, substep graph.
+// Engine behind the C-ABI handle: device memory, stream, substep graphs.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -13,11 +13,14 @@ namespace mpm {
 
 int write_bgeo(const char* path, const float* x, int64_t n, int dim);
 
+struct Chunk;
+
 struct Engine {
     int dim = 3;
     int device = 0;
     cudaStream_t stream = nullptr;
     mpm_options opt{};
+    int num_sms = 148;
 
     // host copies of the tables
     std::vector<SceneParams> scenes_h;
@@ -28,21 +31,39 @@ struct Engine {
     int n_planes = 0;
     long long total_blocks = 0;
 
-    // device memory
-    float* state = nullptr;      // current particle planes
-    float* state_alt = nullptr;  // scratch / sort target
-    uint16_t* grp = nullptr;
-    uint16_t* grp_alt = nullptr;
-    uint32_t* id = nullptr;
-    uint32_t* id_alt = nullptr;
+    // particle state: two buffers (sorted / re-binning target)
+    int cur = 0;
+    float* st[2] = {nullptr, nullptr};
+    uint16_t* gp[2] = {nullptr, nullptr};
+    uint32_t* ids[2] = {nullptr, nullptr};
+
     GroupParams* groups_d = nullptr;
     SceneParams* scenes_d = nullptr;
     float4* grid_mom = nullptr;  // P2G accumulation (momentum, mass)
     float4* grid_vel = nullptr;  // after the grid update (velocity, mass)
     unsigned* err_d = nullptr;
 
-    cudaGraphExec_t graph_exec = nullptr;
-    bool graph_dirty = true;
+    // binning and block activity
+    int* key = nullptr;
+    int* rank = nullptr;
+    int* blk_count = nullptr;
+    int* blk_start = nullptr;
+    void* scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
+    Chunk* chunks = nullptr;
+    long long max_chunks = 0;
+    int* counters = nullptr;  // [0] n_chunks [1] n_active [2] epoch [3] chunk cursor [4] fallback
+    unsigned* blk_flag = nullptr;
+    int* active = nullptr;
+    int* blk_epoch = nullptr;
+    float* pos_out = nullptr;  // gathered positions (creation order)
+    int fused_ctas = 0;
+    int update_ctas = 0;
+    int steps_since_rebin = 0;
+
+    // substep graphs: [parity][rebin first]
+    cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    bool grid_dirty = true;  // grid_mom does not hold the P2G of the current state
 
     double current_time = 0.0;
     long long current_frame = 0;
@@ -61,13 +82,20 @@ struct Engine {
     int count_active_nodes(int scene, int64_t* n);
     int set_p2g_mode(int mode);
     int profile_stages(int n, float* out_ms, int n_out, int* n_written);
+    int get_positions(int scene, float* out);
+    int bin_stats(int64_t* fallbacks, int64_t* rebins);
 
    private:
     int cuda_fail(cudaError_t e, const char* what);
-    void enqueue_substep();
-    int build_graph();
-    void drop_graph();
+    ParticleBuf buf(int p) const { return ParticleBuf{st[p], cap, gp[p], ids[p]}; }
+    void enqueue_direct_substep();
+    void enqueue_rebin(int from);
+    void enqueue_fused_substep(int parity);
+    int prologue();
+    int build_graph(int parity, int rebin);
+    void drop_graphs();
     int unpermute_to_alt();
+    bool fused() const { return opt.p2g_mode == MPM_P2G_ATOMIC; }
 };
 
 }  // namespace mpm

@@ -89,7 +89,8 @@ class Simulation:
     """One C-ABI handle over a list of scenes (all of the same dimension)."""
 
     def __init__(self, scenes: Sequence[Scene], p2g_mode: int = L.P2G_ATOMIC,
-                 stress_mode: int = L.STRESS_PLAIN, use_graph: bool = True, device: int = 0):
+                 stress_mode: int = L.STRESS_PLAIN, use_graph: bool = True, device: int = 0,
+                 rebin_interval: int = 0):
         lib = L.load()
         self.scenes = list(scenes)
         self.dim = self.scenes[0].dim
@@ -132,6 +133,7 @@ class Simulation:
         opt = L.Options()
         lib.mpm_default_options(C.byref(opt))
         opt.p2g_mode, opt.stress_mode, opt.use_graph, opt.device = p2g_mode, stress_mode, int(use_graph), device
+        opt.rebin_interval = rebin_interval
         h = C.c_void_p()
         L.check(lib.mpm_create(sdescs, len(self.scenes), C.byref(opt), C.byref(h)))
         self._h = h
@@ -203,9 +205,13 @@ class Simulation:
         self._check(self._lib.mpm_num_particles(self._h, scene, C.byref(n)))
         return n.value
 
-    def positions(self, scene: int = 0) -> np.ndarray:
+    def positions(self, scene: int = 0, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Positions in creation order.  `out` may be a preallocated (e.g.
+        page-locked) float32 array of shape (n, dim)."""
         n = self.num_particles(scene)
-        out = np.empty((n, self.dim), np.float32)
+        if out is None:
+            out = np.empty((n, self.dim), np.float32)
+        assert out.dtype == np.float32 and out.flags["C_CONTIGUOUS"] and out.size >= n * self.dim
         self._check(self._lib.mpm_get_positions(self._h, scene, L.fptr(out), out.size))
         return out
 
@@ -235,6 +241,12 @@ class Simulation:
         n = C.c_int64()
         self._check(self._lib.mpm_count_active_nodes(self._h, scene, C.byref(n)))
         return n.value
+
+    def bin_stats(self):
+        """(fallback gathers/scatters served from global memory, re-binnings)."""
+        fb, rb = C.c_int64(), C.c_int64()
+        self._check(self._lib.mpm_get_bin_stats(self._h, C.byref(fb), C.byref(rb)))
+        return fb.value, rb.value
 
     def write_bgeo(self, path: str, scene: int = 0):
         self._check(self._lib.mpm_write_bgeo(self._h, scene, path.encode()))

@@ -27,21 +27,27 @@ def blob_scene(d, name, bc=L.BC_SLIP, seed=3, n_grid=32, h=1.0 / 32, ppc=2, radi
                  gravity=(0.0, -9.8, 0.0)[:d] if d == 3 else (0.0, -9.8), **kw)
 
 
+MODES = [L.P2G_ATOMIC, L.P2G_DIRECT]
+MODE_IDS = ["binned", "direct"]
+
+
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
 @pytest.mark.parametrize("d", [2, 3])
 @pytest.mark.parametrize("name", ["jello", "snow", "water"])
-def test_one_substep_matches_oracle(gpu, d, name):
+def test_one_substep_matches_oracle(gpu, d, name, mode):
     sc = blob_scene(d, name)
     orc = oracle_for(sc)
-    with Simulation([sc]) as sim:
+    with Simulation([sc], p2g_mode=mode) as sim:
         sim.step(1)
         got = sim.get_state(0)
     assert orc.step(1) == 0
     compare(got, orc.state(), TOL_STEP)
 
 
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
 @pytest.mark.parametrize("d", [2, 3])
 @pytest.mark.parametrize("bc", [L.BC_STICKY, L.BC_SLIP, L.BC_SEPARATE])
-def test_boundaries_match_oracle(gpu, d, bc):
+def test_boundaries_match_oracle(gpu, d, bc, mode):
     # blob pushed into the lower x wall band so every boundary branch runs
     sc = blob_scene(d, "jello", bc=bc, seed=4)
     g = sc.groups[0]
@@ -49,7 +55,7 @@ def test_boundaries_match_oracle(gpu, d, bc):
     g.v[:, 0] = -np.abs(g.v[:, 0]) - 1.0
     sc.bc_lo, sc.bc_hi = 8, 3
     orc = oracle_for(sc)
-    with Simulation([sc]) as sim:
+    with Simulation([sc], p2g_mode=mode) as sim:
         sim.step(1)
         got = sim.get_state(0)
         mass, vel = sim.get_grid(0)
@@ -60,10 +66,11 @@ def test_boundaries_match_oracle(gpu, d, bc):
     assert rel_err(mass, orc.mass) < 1e-5
 
 
-def test_grid_matches_oracle(gpu):
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
+def test_grid_matches_oracle(gpu, mode):
     sc = blob_scene(3, "snow", seed=8)
     orc = oracle_for(sc)
-    with Simulation([sc]) as sim:
+    with Simulation([sc], p2g_mode=mode) as sim:
         sim.step(1)
         mass, vel = sim.get_grid(0)
         active = sim.count_active_nodes(0)
@@ -73,11 +80,12 @@ def test_grid_matches_oracle(gpu):
     assert active == int((orc.mass > 0).sum())
 
 
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
 @pytest.mark.parametrize("name", ["jello", "snow", "water"])
-def test_twenty_substeps_track_oracle(gpu, name):
+def test_twenty_substeps_track_oracle(gpu, name, mode):
     sc = blob_scene(3, name, seed=21)
     orc = oracle_for(sc)
-    with Simulation([sc]) as sim:
+    with Simulation([sc], p2g_mode=mode, rebin_interval=4) as sim:
         sim.step(20)
         got = sim.get_state(0)
     assert orc.step(20) == 0
@@ -85,10 +93,11 @@ def test_twenty_substeps_track_oracle(gpu, name):
     compare(got, orc.state(), tol)
 
 
-def test_multi_scene_batch_matches_single(gpu):
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
+def test_multi_scene_batch_matches_single(gpu, mode):
     scs = [blob_scene(3, "jello", seed=30), blob_scene(3, "snow", seed=31, n_grid=40, h=1.0 / 40),
            blob_scene(3, "water", seed=32, n_grid=24, h=1.0 / 24)]
-    with Simulation(scs) as sim:
+    with Simulation(scs, p2g_mode=mode, rebin_interval=2) as sim:
         sim.step(3)
         batched = [sim.get_state(i) for i in range(3)]
     for i, sc in enumerate(scs):
@@ -97,14 +106,15 @@ def test_multi_scene_batch_matches_single(gpu):
         compare(batched[i], orc.state(), {"x": 5e-6, "v": 5e-4, "C": 5e-4, "F": 3e-5, "aux": 3e-5})
 
 
-def test_mixed_groups_in_one_grid(gpu):
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
+def test_mixed_groups_in_one_grid(gpu, mode):
     a = blob_scene(3, "jello", seed=40)
     b = blob_scene(3, "water", seed=41)
     for g in b.groups:
         g.x[:, 0] += np.float32(3 * a.h)
     a.groups += b.groups
     orc = oracle_for(a)
-    with Simulation([a]) as sim:
+    with Simulation([a], p2g_mode=mode) as sim:
         sim.step(2)
         got = sim.get_state(0)
     assert orc.step(2) == 0
@@ -202,11 +212,12 @@ def golden_scene(z):
                  gravity=(0.0, -9.8, 0.0), mass_eps=2.220446049250313e-16)
 
 
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
 @pytest.mark.parametrize("path", _golden_files(), ids=lambda p: os.path.basename(p))
-def test_matches_reference_build_golden(gpu, path):
+def test_matches_reference_build_golden(gpu, path, mode):
     z = np.load(path)
     sc = golden_scene(z)
-    with Simulation([sc]) as sim:
+    with Simulation([sc], p2g_mode=mode, rebin_interval=3) as sim:
         done = 0
         for k in (1, 10):
             sim.step(k - done)
@@ -219,3 +230,53 @@ def test_matches_reference_build_golden(gpu, path):
                 got = {f: st[f][off:off + n] for f in st}
                 compare(got, ref, TOL_REF[k])
                 off += n
+
+
+def test_fast_particles_cross_blocks_between_rebinnings(gpu):
+    """Particles moving ~0.4 cells per substep with re-binning only every 32
+    substeps leave their block's tile: those gathers and scatters go to
+    global memory and the result still tracks the oracle."""
+    sc = blob_scene(3, "jello", seed=90)
+    g = sc.groups[0]
+    g.v[:] = np.float32([1.2, -0.8, 0.6]) * np.float32(0.4 * sc.h / sc.dt / 1.2)
+    g.C[:] = 0
+    orc = oracle_for(sc)
+    with Simulation([sc], rebin_interval=32) as sim:
+        sim.step(12)
+        got = sim.get_state(0)
+        fallbacks, rebins = sim.bin_stats()
+    assert orc.step(12) == 0
+    compare(got, orc.state(), {"x": 2e-5, "v": 2e-3, "C": 5e-3, "F": 1e-4, "aux": 1e-4})
+    assert fallbacks > 0
+    assert rebins == 1  # the prologue's
+
+
+def test_switching_modes_keeps_state(gpu):
+    sc = blob_scene(3, "snow", seed=91)
+    orc = oracle_for(sc)
+    with Simulation([sc]) as sim:
+        sim.step(3)
+        sim.set_p2g_mode(L.P2G_DIRECT)
+        sim.step(3)
+        sim.set_p2g_mode(L.P2G_ATOMIC)
+        sim.step(3)
+        got = sim.get_state(0)
+    assert orc.step(9) == 0
+    compare(got, orc.state(), {"x": 5e-6, "v": 1e-3, "C": 1e-3, "F": 5e-5, "aux": 5e-5})
+
+
+def test_set_state_mid_run_binned(gpu):
+    sc = blob_scene(3, "jello", seed=92)
+    with Simulation([sc], rebin_interval=5) as sim:
+        sim.step(7)
+        st = sim.get_state(0)
+        st["v"][:, 0] += np.float32(0.5)
+        sim.set_state(0, v=st["v"])
+        sim.step(2)
+        got = sim.get_state(0)
+    sc2 = blob_scene(3, "jello", seed=92)
+    g = sc2.groups[0]
+    g.x, g.v, g.C, g.F, g.aux = st["x"], st["v"], st["C"], st["F"], st["aux"]
+    orc = oracle_for(sc2)
+    assert orc.step(2) == 0
+    compare(got, orc.state(), {"x": 5e-6, "v": 5e-4, "C": 5e-4, "F": 3e-5, "aux": 3e-5})
