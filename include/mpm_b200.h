@@ -139,6 +139,9 @@ typedef struct mpm_options {
     int device;         /* CUDA device ordinal */
     int rebin_interval; /* substeps between re-binnings of the particles
                            (MPM_P2G_ATOMIC); 0 = tuned default */
+    int kernel_config;  /* fused-kernel launch configuration (chunk size and
+                           CTAs per SM, see mpm_num_kernel_configs); -1 =
+                           choose with the autotuner at creation */
 } mpm_options;
 
 typedef struct mpm_handle mpm_handle;
@@ -222,6 +225,20 @@ int mpm_profile_stages(mpm_handle *h, int n_substeps, float *out_ms, int n_out,
 
 /* Number of grid nodes with non-zero mass in one scene after the last step. */
 int mpm_count_active_nodes(mpm_handle *h, int scene, int64_t *n);
+
+/* Launch configurations of the fused substep kernel (the autotuner's search
+ * space): configuration i runs chunks of *chunk particles with *chunk threads
+ * per CTA and at least *min_ctas CTAs per SM.  No reference counterpart: the
+ * reference launches fixed 128-thread blocks (MPMCUDA.cu:813-815). */
+int mpm_num_kernel_configs(void);
+int mpm_kernel_config_info(int config, int *chunk, int *min_ctas);
+int mpm_get_kernel_config(mpm_handle *h, int *config);
+int mpm_set_kernel_config(mpm_handle *h, int config);
+
+/* Times n_substeps of every configuration on a copy of the state (the
+ * simulation does not advance), keeps the fastest and caches it for handles
+ * of the same shape in this process.  *chosen / *ms_per_substep may be NULL. */
+int mpm_autotune(mpm_handle *h, int n_substeps, int *chosen, float *ms_per_substep);
 
 /* Diagnostics of the binned path: *fallbacks counts particle gathers or
  * scatters that left their block's shared-memory tile (served from global

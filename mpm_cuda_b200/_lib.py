@@ -47,7 +47,8 @@ class SceneDesc(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("p2g_mode", C.c_int), ("stress_mode", C.c_int), ("use_graph", C.c_int),
-                ("block_threads", C.c_int), ("device", C.c_int), ("rebin_interval", C.c_int)]
+                ("block_threads", C.c_int), ("device", C.c_int), ("rebin_interval", C.c_int),
+                ("kernel_config", C.c_int)]
 
 
 EXPORTS = {
@@ -74,6 +75,11 @@ EXPORTS = {
     "mpm_profile_stages": (C.c_int, [C.c_void_p, C.c_int, _FP, C.c_int, C.POINTER(C.c_int)]),
     "mpm_count_active_nodes": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]),
     "mpm_get_bin_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "mpm_num_kernel_configs": (C.c_int, []),
+    "mpm_kernel_config_info": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "mpm_get_kernel_config": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "mpm_set_kernel_config": (C.c_int, [C.c_void_p, C.c_int]),
+    "mpm_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
 }
 
 _lib = None

@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include "mpm_config.cuh"
 #include "mpm_engine.cuh"
 
 namespace {
@@ -50,6 +51,7 @@ void mpm_default_options(mpm_options* opt) {
     opt->block_threads = 0;
     opt->device = 0;
     opt->rebin_interval = 0;
+    opt->kernel_config = -1;
 }
 
 int mpm_create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options* opt,
@@ -166,6 +168,37 @@ int mpm_count_active_nodes(mpm_handle* h, int scene, int64_t* n) {
 int mpm_get_bin_stats(mpm_handle* h, int64_t* fallbacks, int64_t* rebins) {
     if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_get_bin_stats: NULL handle");
     return h->eng.bin_stats(fallbacks, rebins);
+}
+
+int mpm_num_kernel_configs(void) { return mpm::kNumFusedCfgs; }
+
+int mpm_kernel_config_info(int config, int* chunk, int* min_ctas) {
+    if (config < 0 || config >= mpm::kNumFusedCfgs)
+        return fail(nullptr, MPM_ERR_INVALID, "mpm_kernel_config_info: config %d out of range", config);
+    if (chunk) *chunk = mpm::kFusedCfgs[config].chunk;
+    if (min_ctas) *min_ctas = mpm::kFusedCfgs[config].min_ctas;
+    return MPM_OK;
+}
+
+int mpm_get_kernel_config(mpm_handle* h, int* config) {
+    if (!h || !config) return fail(h, MPM_ERR_INVALID, "mpm_get_kernel_config: bad argument");
+    *config = h->eng.cfg;
+    return MPM_OK;
+}
+
+int mpm_set_kernel_config(mpm_handle* h, int config) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_set_kernel_config: NULL handle");
+    if (config < 0 || config >= mpm::kNumFusedCfgs)
+        return fail(h, MPM_ERR_INVALID, "mpm_set_kernel_config: config %d out of range", config);
+    h->eng.set_config(config);
+    return MPM_OK;
+}
+
+int mpm_autotune(mpm_handle* h, int n_substeps, int* chosen, float* ms_per_substep) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_autotune: NULL handle");
+    int rc = h->eng.autotune(n_substeps, ms_per_substep);
+    if (rc == MPM_OK && chosen) *chosen = h->eng.cfg;
+    return rc;
 }
 
 int mpm_get_time(mpm_handle* h, double* t, int64_t* frame) {

@@ -2,12 +2,15 @@
 // launch sequences (binned fused path, unbinned path).
 #include "mpm_engine.cuh"
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include "mpm_kernels_binned.cuh"
 #include "mpm_kernels_direct.cuh"
@@ -18,7 +21,9 @@ namespace {
 
 constexpr int kMaxGroups = 65535;
 constexpr int kDefaultRebinInterval = 16;
-enum { CNT_CHUNKS = 0, CNT_ACTIVE = 1, CNT_EPOCH = 2, CNT_CURSOR = 3, CNT_FALLBACK = 4, CNT_REBINS = 5, CNT_N = 8 };
+// device counters: chunk list lengths and cursors per material, active
+// block count, grid epoch, tile fallbacks, re-binnings
+enum { CNT_CHUNKS = 0, CNT_ACTIVE = 3, CNT_EPOCH = 4, CNT_CURSOR = 5, CNT_FALLBACK = 8, CNT_REBINS = 9, CNT_N = 16 };
 
 // out[id[i]] = in[i] for every plane (storage order -> creation order)
 __global__ void k_unpermute(const float* __restrict__ in, float* __restrict__ out, const uint32_t* __restrict__ id,
@@ -53,11 +58,56 @@ unsigned grid_blocks(long long n, int threads) { return (unsigned)std::max<long 
 
 }  // namespace
 
+// the fused kernel instantiations, indexed [material][config]
+template <int D, int MAT, int CI>
+static constexpr auto fused_kernel() {
+    return &k_g2p2g<D, MAT, kFusedCfgs[CI].chunk, kFusedCfgs[CI].min_ctas, kFusedCfgs[CI].scatter>;
+}
+
+template <int D, int MAT>
+static void (*fused_for(int ci))(ParticleBuf, FusedArgs) {
+    static_assert(kNumFusedCfgs == 8, "update the dispatch table");
+    switch (ci) {
+        case 0: return fused_kernel<D, MAT, 0>();
+        case 1: return fused_kernel<D, MAT, 1>();
+        case 2: return fused_kernel<D, MAT, 2>();
+        case 3: return fused_kernel<D, MAT, 3>();
+        case 4: return fused_kernel<D, MAT, 4>();
+        case 5: return fused_kernel<D, MAT, 5>();
+        case 6: return fused_kernel<D, MAT, 6>();
+        default: return fused_kernel<D, MAT, 7>();
+    }
+}
+
+template <int D>
+static void (*fused_for_mat(int mat, int ci))(ParticleBuf, FusedArgs) {
+    if (mat == JELLO) return fused_for<D, JELLO>(ci);
+    if (mat == SNOW) return fused_for<D, SNOW>(ci);
+    return fused_for<D, WATER>(ci);
+}
+
+static void (*fused_fn(int dim, int mat, int ci))(ParticleBuf, FusedArgs) {
+    return dim == 3 ? fused_for_mat<3>(mat, ci) : fused_for_mat<2>(mat, ci);
+}
+
 int Engine::cuda_fail(cudaError_t e, const char* what) {
     char buf[512];
     std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
     last_error = buf;
     return e == cudaErrorMemoryAllocation ? MPM_ERR_NOMEM : MPM_ERR_CUDA;
+}
+
+// records the first failing launch (by name) since the last take_launch_error()
+void Engine::note_launch(const char* what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess && launch_error.empty()) launch_error = std::string(what) + ": " + cudaGetErrorString(e);
+}
+
+int Engine::take_launch_error() {
+    if (launch_error.empty()) return MPM_OK;
+    last_error = launch_error;
+    launch_error.clear();
+    return MPM_ERR_CUDA;
 }
 
 #define MPM_CUDA_TRY(expr, what)                           \
@@ -245,18 +295,27 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     if ((rc = alloc((void**)&grid_mom, grid_bytes, "grid_mom")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&grid_vel, grid_bytes, "grid_vel")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&err_d, sizeof(unsigned), "err")) != MPM_OK) return rc;
-    if ((rc = alloc((void**)&key, cap * sizeof(int), "key")) != MPM_OK) return rc;
-    if ((rc = alloc((void**)&rank, cap * sizeof(int), "rank")) != MPM_OK) return rc;
-    if ((rc = alloc((void**)&blk_count, total_blocks * sizeof(int), "blk_count")) != MPM_OK) return rc;
-    if ((rc = alloc((void**)&blk_start, total_blocks * sizeof(int), "blk_start")) != MPM_OK) return rc;
+    for (int p = 0; p < 2; ++p) {
+        if ((rc = alloc((void**)&keys[p], cap * sizeof(unsigned long long), "sort keys")) != MPM_OK) return rc;
+        if ((rc = alloc((void**)&vals[p], cap * sizeof(unsigned), "sort values")) != MPM_OK) return rc;
+    }
+    if ((rc = alloc((void**)&cell_count, total_blocks * 64 * sizeof(int), "cell counts")) != MPM_OK) return rc;
+    if ((rc = alloc((void**)&seg_count, total_blocks * 4 * sizeof(int), "segment counts")) != MPM_OK) return rc;
+    if ((rc = alloc((void**)&seg_start, total_blocks * 4 * sizeof(int), "segment starts")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&blk_flag, total_blocks * sizeof(unsigned), "blk_flag")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&active, total_blocks * sizeof(int), "active")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&blk_epoch, total_blocks * sizeof(int), "blk_epoch")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&counters, CNT_N * sizeof(int), "counters")) != MPM_OK) return rc;
-    max_chunks = cap / kChunk + std::min<long long>(cap, total_blocks) + 1;
-    if ((rc = alloc((void**)&chunks, max_chunks * sizeof(Chunk), "chunks")) != MPM_OK) return rc;
-    cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp_bytes, blk_count, blk_start, (int)total_blocks);
+    list_cap = cap / kFusedCfgs[kNumFusedCfgs - 1].chunk + std::min<long long>(cap, total_blocks) + 1;
+    if ((rc = alloc((void**)&chunks, kMats * list_cap * sizeof(Chunk), "chunks")) != MPM_OK) return rc;
+    key_bits = 12;
+    while (key_bits < 64 && (1LL << (key_bits - 12)) < total_blocks) ++key_bits;
+    cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp_bytes, keys[0], keys[1], vals[0], vals[1], (int)cap, 0,
+                                    key_bits);
+    if ((rc = alloc(&sort_tmp, sort_tmp_bytes, "sort temp")) != MPM_OK) return rc;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp_bytes, seg_count, seg_start, (int)(total_blocks * 4));
     if ((rc = alloc(&scan_tmp, scan_tmp_bytes, "scan temp")) != MPM_OK) return rc;
+    for (const GroupParams& g : groups_h) mat_present[g.type] = true;
     if ((rc = alloc((void**)&pos_out, cap * D * sizeof(float), "positions")) != MPM_OK) return rc;
 
     e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
@@ -275,6 +334,8 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     if (e == cudaSuccess) e = cudaMemset(grid_vel, 0, grid_bytes);
     if (e == cudaSuccess) e = cudaMemset(err_d, 0, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(blk_flag, 0, total_blocks * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(cell_count, 0, total_blocks * 64 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(seg_count, 0, total_blocks * 4 * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(blk_epoch, 0xff, total_blocks * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(counters, 0, CNT_N * sizeof(int));
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -282,16 +343,151 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
         msg = std::string("mpm_create: upload: ") + cudaGetErrorString(e);
         return MPM_ERR_CUDA;
     }
-    int per_sm = 0;
-    if (dim == 3)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_g2p2g<3>, kChunk, 0);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_g2p2g<2>, kChunk, 0);
-    fused_ctas = num_sms * std::max(1, per_sm);
-    update_ctas = (int)std::min<long long>((total_blocks + 3) / 4, (long long)num_sms * 8);
+    update_ctas = (int)std::max<long long>(1, std::min<long long>((total_blocks + 3) / 4, (long long)num_sms * 8));
+    cfg = (opt.kernel_config >= 0 && opt.kernel_config < kNumFusedCfgs) ? opt.kernel_config : 1;
+    set_config(cfg);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        msg = std::string("mpm_create: pending CUDA error: ") + cudaGetErrorString(e);
+        return MPM_ERR_CUDA;
+    }
+    if (opt.kernel_config < 0 && n_particles > 0) {
+        const int cached = cached_config();
+        if (cached >= 0) {
+            set_config(cached);
+        } else {
+            const int trc = autotune(8, nullptr);
+            if (trc != MPM_OK) {
+                msg = "mpm_create: autotune: " + last_error;
+                return trc;
+            }
+        }
+    }
     cur = 0;
     grid_dirty = true;
     return MPM_OK;
+}
+
+void Engine::set_config(int ci) {
+    cfg = ci;
+    for (int mat = 0; mat < kMats; ++mat) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_fn(dim, mat, ci), kFusedCfgs[ci].chunk, 0) !=
+            cudaSuccess) {
+            cudaGetLastError();  // the query failed: fall back to one CTA per SM
+            per_sm = 1;
+        }
+        fused_ctas[mat] = num_sms * std::max(1, per_sm);
+    }
+    drop_graphs();
+    grid_dirty = true;  // chunk lists depend on the chunk size
+}
+
+namespace {
+
+// autotuner results of this process, keyed by the workload's shape
+struct TuneKey {
+    int device, dim, mats;
+    long long particles, blocks;
+    bool operator<(const TuneKey& o) const {
+        if (device != o.device) return device < o.device;
+        if (dim != o.dim) return dim < o.dim;
+        if (mats != o.mats) return mats < o.mats;
+        if (particles != o.particles) return particles < o.particles;
+        return blocks < o.blocks;
+    }
+};
+std::map<TuneKey, int>& tune_cache() {
+    static std::map<TuneKey, int> m;
+    return m;
+}
+std::mutex& tune_mutex() {
+    static std::mutex m;
+    return m;
+}
+
+}  // namespace
+
+// Times `steps` substeps of every fused-kernel configuration on a copy of
+// the current state and keeps the fastest; the state, clock and counters are
+// restored afterwards, so tuning does not advance the simulation.
+int Engine::autotune(int steps, float* best_ms) {
+    MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    if (steps <= 0) steps = 8;
+    const size_t state_bytes = (size_t)n_planes * cap * sizeof(float);
+    float* bk_state = nullptr;
+    uint16_t* bk_grp = nullptr;
+    uint32_t* bk_id = nullptr;
+    cudaError_t e = cudaMalloc((void**)&bk_state, state_bytes);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&bk_grp, cap * sizeof(uint16_t));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&bk_id, cap * sizeof(uint32_t));
+    unsigned err_before = 0;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) e = cudaMemcpy(&err_before, err_d, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(bk_state, st[cur], state_bytes, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(bk_grp, gp[cur], cap * sizeof(uint16_t), cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(bk_id, ids[cur], cap * sizeof(uint32_t), cudaMemcpyDeviceToDevice);
+    const double t0 = current_time;
+    const long long f0 = current_frame;
+    const int mode0 = opt.p2g_mode;
+    opt.p2g_mode = MPM_P2G_ATOMIC;
+    int best = cfg;
+    float best_t = 1e30f;
+    int rc = MPM_OK;
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    for (int ci = 0; ci < kNumFusedCfgs && e == cudaSuccess && rc == MPM_OK; ++ci) {
+        e = cudaMemcpyAsync(st[cur], bk_state, state_bytes, cudaMemcpyDeviceToDevice, stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(gp[cur], bk_grp, cap * sizeof(uint16_t), cudaMemcpyDeviceToDevice, stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(ids[cur], bk_id, cap * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream);
+        if (e != cudaSuccess) break;
+        set_config(ci);
+        if ((rc = step(2)) != MPM_OK) break;  // prologue, graph capture, warm-up
+        cudaEventRecord(a, stream);
+        if ((rc = step(steps)) != MPM_OK) break;
+        cudaEventRecord(b, stream);
+        e = cudaEventSynchronize(b);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+        if (e == cudaSuccess && ms < best_t) {
+            best_t = ms;
+            best = ci;
+        }
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    // restore
+    cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) e = cudaMemcpy(st[cur], bk_state, state_bytes, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(gp[cur], bk_grp, cap * sizeof(uint16_t), cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(ids[cur], bk_id, cap * sizeof(uint32_t), cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(err_d, &err_before, sizeof(unsigned), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(counters + CNT_FALLBACK, 0, 2 * sizeof(int));
+    cudaFree(bk_state);
+    cudaFree(bk_grp);
+    cudaFree(bk_id);
+    opt.p2g_mode = mode0;
+    current_time = t0;
+    current_frame = f0;
+    set_config(best);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "autotune");
+    if (rc != MPM_OK) return rc;
+    if (best_ms) *best_ms = best_t / steps;
+    int mats = 0;
+    for (int m = 0; m < kMats; ++m) mats |= mat_present[m] ? (1 << m) : 0;
+    std::lock_guard<std::mutex> lk(tune_mutex());
+    tune_cache()[TuneKey{device, dim, mats, n_particles, total_blocks}] = best;
+    return MPM_OK;
+}
+
+int Engine::cached_config() const {
+    int mats = 0;
+    for (int m = 0; m < kMats; ++m) mats |= mat_present[m] ? (1 << m) : 0;
+    std::lock_guard<std::mutex> lk(tune_mutex());
+    auto it = tune_cache().find(TuneKey{device, dim, mats, n_particles, total_blocks});
+    return it == tune_cache().end() ? -1 : it->second;
 }
 
 void Engine::release() {
@@ -306,14 +502,18 @@ void Engine::release() {
         gp[p] = nullptr;
         ids[p] = nullptr;
     }
-    void* ptrs[] = {groups_d, scenes_d, grid_mom, grid_vel, err_d, key, rank, blk_count, blk_start,
-                    blk_flag, active, blk_epoch, counters, chunks, scan_tmp, pos_out};
+    void* ptrs[] = {groups_d, scenes_d, grid_mom, grid_vel, err_d, keys[0], keys[1], vals[0], vals[1],
+                    cell_count, seg_count, seg_start, sort_tmp, blk_flag, active, blk_epoch, counters, chunks,
+                    scan_tmp, pos_out};
     for (void* p : ptrs) cudaFree(p);
     groups_d = nullptr;
     scenes_d = nullptr;
     grid_mom = grid_vel = nullptr;
     err_d = nullptr;
-    key = rank = blk_count = blk_start = nullptr;
+    keys[0] = keys[1] = nullptr;
+    vals[0] = vals[1] = nullptr;
+    cell_count = seg_count = seg_start = nullptr;
+    sort_tmp = nullptr;
     blk_flag = nullptr;
     active = blk_epoch = counters = nullptr;
     chunks = nullptr;
@@ -359,35 +559,64 @@ void Engine::enqueue_direct_substep() {
     }
 }
 
-// counting sort of the particles of buffer `from` by home block into the
-// other buffer, and the chunk table of the result
+// radix sort of the particles of buffer `from` by (home block, material,
+// rank in cell, cell) into the other buffer, and the chunk lists of the result
 void Engine::enqueue_rebin(int from) {
     const int to = 1 - from;
-    cudaMemsetAsync(blk_count, 0, total_blocks * sizeof(int), stream);
-    cudaMemsetAsync(counters + CNT_CHUNKS, 0, sizeof(int), stream);
+    const long long n_segs = total_blocks * 4;
+    cudaMemsetAsync(counters + CNT_CHUNKS, 0, kMats * sizeof(int), stream);
     if (n_particles > 0) {
         if (dim == 3)
-            k_bin_count<3><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), n_particles, groups_d,
-                                                                              scenes_d, key, rank, blk_count);
+            k_bin_key<3><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d,
+                                                                            keys[0], vals[0], cell_count, seg_count);
         else
-            k_bin_count<2><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), n_particles, groups_d,
-                                                                              scenes_d, key, rank, blk_count);
-    }
-    cub::DeviceScan::ExclusiveSum(scan_tmp, scan_tmp_bytes, blk_count, blk_start, (int)total_blocks, stream);
-    if (n_particles > 0) {
+            k_bin_key<2><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d,
+                                                                            keys[0], vals[0], cell_count, seg_count);
+        note_launch("k_bin_key");
+        cub::DeviceRadixSort::SortPairs(sort_tmp, sort_tmp_bytes, keys[0], keys[1], vals[0], vals[1],
+                                        (int)n_particles, 0, key_bits, stream);
+        note_launch("cub::DeviceRadixSort::SortPairs");
         if (dim == 3)
-            k_bin_scatter<3><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), buf(to), n_particles, key,
-                                                                                rank, blk_start);
+            k_bin_gather<3><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), buf(to), n_particles,
+                                                                               vals[1]);
         else
-            k_bin_scatter<2><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), buf(to), n_particles, key,
-                                                                                rank, blk_start);
+            k_bin_gather<2><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), buf(to), n_particles,
+                                                                               vals[1]);
+        note_launch("k_bin_gather");
     }
-    k_make_chunks<<<grid_blocks(total_blocks, 256), 256, 0, stream>>>(blk_count, blk_start, total_blocks, chunks,
-                                                                      counters + CNT_CHUNKS);
+    cub::DeviceScan::ExclusiveSum(scan_tmp, scan_tmp_bytes, seg_count, seg_start, (int)n_segs, stream);
+    note_launch("cub::DeviceScan::ExclusiveSum");
+    k_make_chunks<<<grid_blocks(n_segs, 256), 256, 0, stream>>>(seg_count, seg_start, n_segs, chunks, list_cap,
+                                                                counters + CNT_CHUNKS, kFusedCfgs[cfg].chunk);
+    note_launch("k_make_chunks");
+    if (n_particles > 0)
+        k_bin_reset<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys[1], n_particles, cell_count, seg_count);
+    note_launch("k_bin_reset");
     k_count_rebin<<<1, 1, 0, stream>>>(counters + CNT_REBINS);
+    note_launch("k_count_rebin");
 }
 
-void Engine::enqueue_fused_substep(int parity) {
+FusedArgs Engine::fused_args(int mat, bool bump) {
+    FusedArgs A;
+    A.chunks = chunks + mat * list_cap;
+    A.n_chunks = counters + CNT_CHUNKS + mat;
+    A.cursor = counters + CNT_CURSOR + mat;
+    A.groups = groups_d;
+    A.scenes = scenes_d;
+    A.n_scenes = (int)scenes_h.size();
+    A.grid_vel = grid_vel;
+    A.grid_mom = grid_mom;
+    A.blk_flag = blk_flag;
+    A.active = active;
+    A.n_active = counters + CNT_ACTIVE;
+    A.epoch = counters + CNT_EPOCH;
+    A.bump_epoch = bump ? 1 : 0;
+    A.err_word = err_d;
+    A.fallback = (unsigned*)(counters + CNT_FALLBACK);
+    return A;
+}
+
+void Engine::enqueue_grid_update() {
     const int n_scenes = (int)scenes_h.size();
     if (dim == 3)
         k_grid_update_active<3><<<update_ctas, 256, 0, stream>>>(grid_mom, grid_vel, active, counters + CNT_ACTIVE,
@@ -397,27 +626,26 @@ void Engine::enqueue_fused_substep(int parity) {
         k_grid_update_active<2><<<update_ctas, 256, 0, stream>>>(grid_mom, grid_vel, active, counters + CNT_ACTIVE,
                                                                  blk_flag, blk_epoch, counters + CNT_EPOCH, scenes_d,
                                                                  n_scenes);
+    note_launch("k_grid_update_active");
+    // the fused launches append the blocks of the next substep from zero
     cudaMemsetAsync(counters + CNT_ACTIVE, 0, sizeof(int), stream);
-    cudaMemsetAsync(counters + CNT_CURSOR, 0, sizeof(int), stream);
-    FusedArgs A;
-    A.chunks = chunks;
-    A.n_chunks = counters + CNT_CHUNKS;
-    A.cursor = counters + CNT_CURSOR;
-    A.groups = groups_d;
-    A.scenes = scenes_d;
-    A.n_scenes = n_scenes;
-    A.grid_vel = grid_vel;
-    A.grid_mom = grid_mom;
-    A.blk_flag = blk_flag;
-    A.active = active;
-    A.n_active = counters + CNT_ACTIVE;
-    A.epoch = counters + CNT_EPOCH;
-    A.err_word = err_d;
-    A.fallback = (unsigned*)(counters + CNT_FALLBACK);
-    if (dim == 3)
-        k_g2p2g<3><<<fused_ctas, kChunk, 0, stream>>>(buf(parity), A);
-    else
-        k_g2p2g<2><<<fused_ctas, kChunk, 0, stream>>>(buf(parity), A);
+    cudaMemsetAsync(counters + CNT_CURSOR, 0, kMats * sizeof(int), stream);
+}
+
+void Engine::enqueue_g2p2g(int parity) {
+    bool bump = true;
+    for (int mat = 0; mat < kMats; ++mat) {
+        if (!mat_present[mat]) continue;
+        const FusedArgs A = fused_args(mat, bump);
+        bump = false;
+        fused_fn(dim, mat, cfg)<<<fused_ctas[mat], kFusedCfgs[cfg].chunk, 0, stream>>>(buf(parity), A);
+        note_launch("fused_fn");
+    }
+}
+
+void Engine::enqueue_fused_substep(int parity) {
+    enqueue_grid_update();
+    enqueue_g2p2g(parity);
 }
 
 // makes grid_mom hold the P2G of the current state (binned path): sorts the
@@ -438,7 +666,9 @@ int Engine::prologue() {
             k_p2g_prologue<2><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(
                 buf(cur), n_particles, groups_d, scenes_d, grid_mom, blk_flag, active, counters + CNT_ACTIVE, err_d);
     }
-    MPM_CUDA_TRY(cudaGetLastError(), "prologue launch");
+    note_launch("k_p2g_prologue");
+    int lrc = take_launch_error();
+    if (lrc != MPM_OK) return lrc;
     grid_dirty = false;
     return MPM_OK;
 }
@@ -455,7 +685,12 @@ int Engine::build_graph(int parity, int rebin) {
     cudaError_t e = cudaStreamEndCapture(stream, &g);
     if (e != cudaSuccess) {
         if (g) cudaGraphDestroy(g);
+        take_launch_error();
         return cuda_fail(e, "graph capture end");
+    }
+    if (take_launch_error() != MPM_OK) {
+        cudaGraphDestroy(g);
+        return MPM_ERR_CUDA;
     }
     e = cudaGraphInstantiate(&graphs[parity][rebin], g, 0);
     cudaGraphDestroy(g);
@@ -510,6 +745,8 @@ int Engine::step(int n) {
             } else {
                 if (rebin) enqueue_rebin(cur);
                 enqueue_fused_substep(rebin ? 1 - cur : cur);
+                const int lrc = take_launch_error();
+                if (lrc != MPM_OK) return lrc;
                 MPM_CUDA_TRY(cudaGetLastError(), "kernel launch");
             }
             if (rebin) {
@@ -556,6 +793,7 @@ int Engine::sync_and_check() {
 
 int Engine::unpermute_to_alt() {
     if (n_particles == 0) return MPM_OK;
+    MPM_CUDA_TRY(cudaGetLastError(), "pending error before unpermute");
     k_unpermute<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(st[cur], st[1 - cur], ids[cur], n_particles, cap,
                                                                    n_planes);
     MPM_CUDA_TRY(cudaGetLastError(), "unpermute launch");
@@ -723,42 +961,14 @@ int Engine::profile_stages(int n, float* out_ms, int n_out, int* n_written) {
         acc[0] *= n;
         for (int it = 0; it < n; ++it) {
             cudaEventRecord(ev[0], stream);
-            if (dim == 3)
-                k_grid_update_active<3><<<update_ctas, 256, 0, stream>>>(grid_mom, grid_vel, active,
-                                                                         counters + CNT_ACTIVE, blk_flag, blk_epoch,
-                                                                         counters + CNT_EPOCH, scenes_d, n_scenes);
-            else
-                k_grid_update_active<2><<<update_ctas, 256, 0, stream>>>(grid_mom, grid_vel, active,
-                                                                         counters + CNT_ACTIVE, blk_flag, blk_epoch,
-                                                                         counters + CNT_EPOCH, scenes_d, n_scenes);
+            enqueue_grid_update();
             cudaEventRecord(ev[1], stream);
-            cudaMemsetAsync(counters + CNT_ACTIVE, 0, sizeof(int), stream);
-            cudaMemsetAsync(counters + CNT_CURSOR, 0, sizeof(int), stream);
+            enqueue_g2p2g(cur);
             cudaEventRecord(ev[2], stream);
-            FusedArgs A;
-            A.chunks = chunks;
-            A.n_chunks = counters + CNT_CHUNKS;
-            A.cursor = counters + CNT_CURSOR;
-            A.groups = groups_d;
-            A.scenes = scenes_d;
-            A.n_scenes = n_scenes;
-            A.grid_vel = grid_vel;
-            A.grid_mom = grid_mom;
-            A.blk_flag = blk_flag;
-            A.active = active;
-            A.n_active = counters + CNT_ACTIVE;
-            A.epoch = counters + CNT_EPOCH;
-            A.err_word = err_d;
-            A.fallback = (unsigned*)(counters + CNT_FALLBACK);
-            if (dim == 3)
-                k_g2p2g<3><<<fused_ctas, kChunk, 0, stream>>>(buf(cur), A);
-            else
-                k_g2p2g<2><<<fused_ctas, kChunk, 0, stream>>>(buf(cur), A);
-            cudaEventRecord(ev[3], stream);
-            cudaEventSynchronize(ev[3]);
+            cudaEventSynchronize(ev[2]);
             float a = 0.f, b = 0.f;
             cudaEventElapsedTime(&a, ev[0], ev[1]);
-            cudaEventElapsedTime(&b, ev[2], ev[3]);
+            cudaEventElapsedTime(&b, ev[1], ev[2]);
             acc[1] += a;
             acc[2] += b;
             ++steps_since_rebin;
@@ -800,6 +1010,8 @@ int Engine::profile_stages(int n, float* out_ms, int n_out, int* n_written) {
         }
     }
     for (auto& e : ev) cudaEventDestroy(e);
+    const int lrc = take_launch_error();
+    if (lrc != MPM_OK) return lrc;
     MPM_CUDA_TRY(cudaGetLastError(), "profile launch");
     const int w = std::min(n_out, 3);
     for (int s = 0; s < w; ++s) out_ms[s] = acc[s] / n;

@@ -14,6 +14,7 @@ namespace mpm {
 int write_bgeo(const char* path, const float* x, int64_t n, int dim);
 
 struct Chunk;
+struct FusedArgs;
 
 struct Engine {
     int dim = 3;
@@ -44,20 +45,26 @@ struct Engine {
     unsigned* err_d = nullptr;
 
     // binning and block activity
-    int* key = nullptr;
-    int* rank = nullptr;
-    int* blk_count = nullptr;
-    int* blk_start = nullptr;
+    unsigned long long* keys[2] = {nullptr, nullptr};  // radix sort keys in / out
+    unsigned* vals[2] = {nullptr, nullptr};            // particle index in / sorted
+    int* cell_count = nullptr;  // per node of every block: particles whose base is that node
+    int* seg_count = nullptr;   // per (block, material)
+    int* seg_start = nullptr;
+    void* sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
     void* scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
-    Chunk* chunks = nullptr;
-    long long max_chunks = 0;
-    int* counters = nullptr;  // [0] n_chunks [1] n_active [2] epoch [3] chunk cursor [4] fallback
+    int key_bits = 64;
+    Chunk* chunks = nullptr;    // kMats lists of list_cap entries
+    long long list_cap = 0;
+    bool mat_present[3] = {false, false, false};
+    int* counters = nullptr;    // see CNT_* in mpm_engine.cu
     unsigned* blk_flag = nullptr;
     int* active = nullptr;
     int* blk_epoch = nullptr;
     float* pos_out = nullptr;  // gathered positions (creation order)
-    int fused_ctas = 0;
+    int fused_ctas[3] = {0, 0, 0};  // persistent CTAs per material kernel
+    int cfg = 1;                     // index into kFusedCfgs
     int update_ctas = 0;
     int steps_since_rebin = 0;
 
@@ -68,6 +75,7 @@ struct Engine {
     double current_time = 0.0;
     long long current_frame = 0;
     std::string last_error;
+    std::string launch_error;  // first failed launch since the last check
 
     int create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options& o, std::string& msg);
     void release();
@@ -84,13 +92,21 @@ struct Engine {
     int profile_stages(int n, float* out_ms, int n_out, int* n_written);
     int get_positions(int scene, float* out);
     int bin_stats(int64_t* fallbacks, int64_t* rebins);
+    void set_config(int ci);
+    int autotune(int steps, float* best_ms);
+    int cached_config() const;
 
    private:
     int cuda_fail(cudaError_t e, const char* what);
+    void note_launch(const char* what);
+    int take_launch_error();
     ParticleBuf buf(int p) const { return ParticleBuf{st[p], cap, gp[p], ids[p]}; }
     void enqueue_direct_substep();
     void enqueue_rebin(int from);
     void enqueue_fused_substep(int parity);
+    void enqueue_grid_update();
+    void enqueue_g2p2g(int parity);
+    FusedArgs fused_args(int mat, bool bump);
     int prologue();
     int build_graph(int parity, int rebin);
     void drop_graphs();

@@ -1,103 +1,152 @@
 // Binned substep: particles sorted by home grid block, one fused kernel per
-// substep that gathers (G2P), updates the particle, evaluates the stress and
-// scatters (P2G) for the next substep through shared-memory grid tiles, and
-// a grid update that visits only the blocks P2G touched.
+// substep and material that gathers (G2P), updates the particle, evaluates
+// the stress and scatters (P2G) for the next substep through shared-memory
+// grid tiles, and a grid update that visits only the blocks P2G touched.
 //
 // Home block: the 4x4x4 node block (8x8 in 2D) that holds a particle's base
-// node at the last re-binning.  A chunk is up to CHUNK particles of one home
-// block, contiguous in the sorted state.  The tile of a chunk is the node
-// window [4b - 1, 4b + 7) per axis: it holds the stencil of every particle
-// whose base node is within one node of the home block.  Particles that
-// drifted further since the last re-binning use global memory directly, so
-// results never depend on how stale the binning is.
+// node at the last re-binning.  Inside a block the particles are ordered by
+// (material, rank inside their cell, cell): a warp's 32 consecutive particles
+// then sit in 32 different cells, so the 32 lanes of every shared-memory
+// scatter hit 32 different nodes, and the tile strides below put those nodes
+// in different banks.  A chunk is up to `chunk` particles of one block and one
+// material, contiguous in the sorted state.  The tile of a chunk is the node
+// window [S b - 1, S b + S + 3) per axis (S = block side): it holds the
+// stencil of every particle whose base node is within one node of the home
+// block.  Particles that drifted further since the last re-binning use global
+// memory directly, so results never depend on how stale the binning is.
 #pragma once
 
+#include "mpm_config.cuh"
 #include "mpm_grid.cuh"
 #include "mpm_kernels_direct.cuh"
 #include "mpm_particle.cuh"
 
 namespace mpm {
 
+constexpr int kMaxChunk = 256;  // largest chunk (particles per fused CTA)
+constexpr int kMaxRank = 15;    // rank-in-cell field of the sort key (4 bits)
+constexpr int kMats = 3;        // JELLO, SNOW, WATER
+
+
 struct Chunk {
-    int block;   // global block index (scene block_off + local block)
-    int start;   // first sorted particle
-    int count;   // particles in this chunk
-    int pad;
+    int block;  // global block index (scene block_off + local block)
+    int start;  // first sorted particle
+    int count;  // particles in this chunk
+    int mat;    // material of every particle of the chunk
 };
 
+// Tile layout.  3D: window 8^3; the velocity tile (float4) has strides
+// (1, 12, 96) so the 8 lanes of an LDS.128 phase (cells x 0..3, y 0..1) read
+// 8 distinct 16-byte bank groups; the momentum planes (float) have strides
+// (1, 8, 68) so 32 lanes on a 4x4x2 cell patch hit 32 distinct banks.
 template <int D>
-struct TileShape {
-    static constexpr int SIDE = BlockShape<D>::SIDE;
-    static constexpr int T = SIDE + 4;                    // window width per axis
-    static constexpr int N = (D == 3) ? T * T * T : T * T; // nodes per tile
+struct TileShape;
+
+template <>
+struct TileShape<3> {
+    static constexpr int SIDE = 4;
+    static constexpr int T = 8;
+    static constexpr int N = 512;
+    static constexpr int VY = 12, VZ = 96, VN = 768;
+    static constexpr int MY = 8, MZ = 68, MN = 7 + 7 * 8 + 7 * 68 + 1;
 };
 
-constexpr int kChunk = 256;  // particles per chunk = threads per fused CTA
+template <>
+struct TileShape<2> {
+    static constexpr int SIDE = 8;
+    static constexpr int T = 12;
+    static constexpr int N = 144;
+    static constexpr int VY = 12, VZ = 0, VN = 144;
+    static constexpr int MY = 12, MZ = 0, MN = 144;
+};
 
 // ------------------------------------------------------------- binning --
 
 template <int D>
-__device__ __forceinline__ long long home_block_of(const SceneParams& sc, const float* x) {
+__device__ __forceinline__ void home_of(const SceneParams& sc, const float* x, long long& blk, int& cell) {
     constexpr int S = BlockShape<D>::SHIFT;
-    int b[3] = {0, 0, 0};
+    constexpr int M = BlockShape<D>::SIDE - 1;
+    int b[3] = {0, 0, 0}, c[3] = {0, 0, 0};
 #pragma unroll
     for (int a = 0; a < D; ++a) {
         const float gx = (x[a] - sc.origin[a]) * sc.inv_h;
         int base = isfinite(gx) ? (int)floorf(gx - 0.5f) : 0;
         base = min(max(base, 0), sc.n[a] - 3);
         b[a] = base >> S;
+        c[a] = base & M;
     }
-    return sc.block_off + (long long)b[0] + (long long)sc.nb[0] * (b[1] + (long long)sc.nb[1] * b[2]);
+    blk = sc.block_off + (long long)b[0] + (long long)sc.nb[0] * (b[1] + (long long)sc.nb[1] * b[2]);
+    cell = c[0] + BlockShape<D>::SIDE * (c[1] + BlockShape<D>::SIDE * c[2]);  // 0..63
 }
 
-// key = home block; rank = arrival order inside the block
+// sort key (block, material, rank in cell, cell) and the identity payload
 template <int D>
-__global__ void __launch_bounds__(256) k_bin_count(ParticleBuf pb, long long n, const GroupParams* __restrict__ groups,
-                                                   const SceneParams* __restrict__ scenes, int* __restrict__ key,
-                                                   int* __restrict__ rank, int* __restrict__ blk_count) {
+__global__ void __launch_bounds__(256) k_bin_key(ParticleBuf pb, long long n, const GroupParams* __restrict__ groups,
+                                                 const SceneParams* __restrict__ scenes,
+                                                 unsigned long long* __restrict__ keys, unsigned* __restrict__ vals,
+                                                 int* __restrict__ cell_count, int* __restrict__ seg_count) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float x[D];
 #pragma unroll
     for (int a = 0; a < D; ++a) x[a] = pb.s[(Planes<D>::X + a) * pb.cap + i];
-    const SceneParams& sc = scenes[groups[pb.grp[i]].scene];
-    const long long b = home_block_of<D>(sc, x);
-    key[i] = (int)b;
-    rank[i] = atomicAdd(&blk_count[b], 1);
+    const GroupParams& g = groups[pb.grp[i]];
+    const SceneParams& sc = scenes[g.scene];
+    long long b;
+    int c;
+    home_of<D>(sc, x, b, c);
+    const int r = min(atomicAdd(&cell_count[b * 64 + c], 1), kMaxRank);
+    atomicAdd(&seg_count[b * 4 + g.type], 1);
+    keys[i] = ((unsigned long long)b << 12) | ((unsigned long long)g.type << 10) | ((unsigned long long)r << 6) |
+              (unsigned long long)c;
+    vals[i] = (unsigned)i;
 }
 
-// moves every particle to blk_start[key] + rank in the other buffer
+// dst[j] = src[perm[j]] for every plane, group and creation index
 template <int D>
-__global__ void __launch_bounds__(256) k_bin_scatter(ParticleBuf src, ParticleBuf dst, long long n,
-                                                     const int* __restrict__ key, const int* __restrict__ rank,
-                                                     const int* __restrict__ blk_start) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const long long j = (long long)blk_start[key[i]] + rank[i];
+__global__ void __launch_bounds__(256) k_bin_gather(ParticleBuf src, ParticleBuf dst, long long n,
+                                                    const unsigned* __restrict__ perm) {
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const long long i = perm[j];
 #pragma unroll
     for (int p = 0; p < Planes<D>::COUNT; ++p) dst.s[p * dst.cap + j] = src.s[p * src.cap + i];
     dst.grp[j] = src.grp[i];
     dst.id[j] = src.id[i];
 }
 
-// one chunk list entry per kChunk particles of every non-empty block
-__global__ void __launch_bounds__(256) k_make_chunks(const int* __restrict__ blk_count, const int* __restrict__ blk_start,
-                                                     long long total_blocks, Chunk* __restrict__ chunks,
-                                                     int* __restrict__ n_chunks) {
-    const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= total_blocks) return;
-    const int c = blk_count[b];
+// one chunk per `chunk` particles of every non-empty (block, material)
+// segment, appended to that material's list
+__global__ void __launch_bounds__(256) k_make_chunks(const int* __restrict__ seg_count,
+                                                     const int* __restrict__ seg_start, long long n_segs,
+                                                     Chunk* __restrict__ chunks, long long list_cap,
+                                                     int* __restrict__ n_chunks, int chunk) {
+    const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_segs) return;
+    const int c = seg_count[s];
     if (c == 0) return;
-    const int nch = (c + kChunk - 1) / kChunk;
-    const int o = atomicAdd(n_chunks, nch);
+    const int mat = (int)(s & 3);
+    const int nch = (c + chunk - 1) / chunk;
+    const int o = atomicAdd(&n_chunks[mat], nch);
     for (int j = 0; j < nch; ++j) {
         Chunk ch;
-        ch.block = (int)b;
-        ch.start = blk_start[b] + j * kChunk;
-        ch.count = min(kChunk, c - j * kChunk);
-        ch.pad = 0;
-        chunks[o + j] = ch;
+        ch.block = (int)(s >> 2);
+        ch.start = seg_start[s] + j * chunk;
+        ch.count = min(chunk, c - j * chunk);
+        ch.mat = mat;
+        chunks[mat * list_cap + o + j] = ch;
     }
+}
+
+// zero the cell and segment counters the last k_bin_key touched
+__global__ void __launch_bounds__(256) k_bin_reset(const unsigned long long* __restrict__ keys, long long n,
+                                                   int* __restrict__ cell_count, int* __restrict__ seg_count) {
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const unsigned long long k = keys[j];
+    const long long b = (long long)(k >> 12);
+    cell_count[b * 64 + (int)(k & 63)] = 0;
+    seg_count[b * 4 + (int)((k >> 10) & 3)] = 0;
 }
 
 __global__ void k_count_rebin(int* counter) { *counter += 1; }
@@ -119,17 +168,9 @@ __device__ __forceinline__ long long block_of_node(const SceneParams& sc, int ix
 template <int D>
 __device__ __forceinline__ void p2g_global(const Stencil<D>& st, const P2GSource<D>& src, const SceneParams& sc,
                                            float4* grid_mom, unsigned* blk_flag, int* active, int* n_active) {
-#pragma unroll
-    for (int ox = 0; ox < 3; ++ox)
-#pragma unroll
-        for (int oy = 0; oy < 3; ++oy)
-#pragma unroll
-            for (int oz = 0; oz < (D == 3 ? 3 : 1); ++oz) {
-                const int o[3] = {ox, oy, oz};
-                const float4 c = p2g_node<D>(st, src, o, sc.h, sc.inv_h);
-                const int ix = st.base[0] + ox, iy = st.base[1] + oy, iz = D == 3 ? st.base[2] + oz : 0;
-                atomicAdd(&grid_mom[node_index<D>(sc, ix, iy, iz)], c);
-            }
+    p2g_scatter<D>(st, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 c) {
+        atomicAdd(&grid_mom[node_index<D>(sc, st.base[0] + ox, st.base[1] + oy, D == 3 ? st.base[2] + oz : 0)], c);
+    });
     // the stencil spans at most 2 blocks per axis: mark its corner blocks
 #pragma unroll
     for (int cx = 0; cx < 2; ++cx)
@@ -199,9 +240,9 @@ __global__ void __launch_bounds__(256) k_grid_update_active(float4* __restrict__
 // ------------------------------------------------------------ G2P2G --
 
 struct FusedArgs {
-    const Chunk* chunks;
-    const int* n_chunks;
-    int* cursor;  // next chunk to hand out (zeroed before every launch)
+    const Chunk* chunks;  // this material's chunk list
+    const int* n_chunks;  // its length
+    int* cursor;          // next chunk to hand out (zeroed before every launch)
     const GroupParams* groups;
     const SceneParams* scenes;
     int n_scenes;
@@ -210,29 +251,46 @@ struct FusedArgs {
     unsigned* blk_flag;
     int* active;
     int* n_active;
-    int* epoch;
+    int* epoch;      // bumped once per substep (by the launch with bump_epoch)
+    int bump_epoch;
     unsigned* err_word;
     unsigned* fallback;  // count of particles that used global memory
 };
 
-// One substep for the particles of each chunk: G2P from the velocity tile,
-// F / Jp / J update, advection, stress, and P2G of the next substep into a
-// shared momentum tile flushed with float4 atomics (MPMCUDA.cu:310-741 in
-// one pass: the reference runs P2G, VelUpdate and InterpolateAndMove as
-// three kernels with full-grid sweeps and host syncs between them).
 template <int D>
-__global__ void __launch_bounds__(kChunk, 2) k_g2p2g(ParticleBuf pb, FusedArgs A) {
+__device__ __forceinline__ int tv_idx(int x, int y, int z) {
+    return x + TileShape<D>::VY * y + TileShape<D>::VZ * z;
+}
+
+template <int D>
+__device__ __forceinline__ int tm_idx(int x, int y, int z) {
+    return x + TileShape<D>::MY * y + TileShape<D>::MZ * z;
+}
+
+// One substep for the particles of each chunk of material MAT: G2P from the
+// velocity tile, F / Jp / J update, advection, stress, and P2G of the next
+// substep (MPMCUDA.cu:310-741 in one pass: the reference runs P2G, VelUpdate
+// and InterpolateAndMove as three kernels with full-grid sweeps and host
+// syncs between them).  Two scatter variants (SCAT):
+//   0  into a shared momentum window with shared-memory atomics; the 32 lanes
+//      of a warp hit 32 different nodes (sort order) in 32 different banks
+//      (window strides); the window is flushed once with float4 atomics
+//   1  straight to global memory with float4 vector reductions
+//      (red.global.add.v4.f32); no momentum window, so more CTAs fit per SM
+template <int D, int MAT, int CHUNK, int MINB, int SCAT>
+__global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs A) {
     using P = Planes<D>;
     using TS = TileShape<D>;
     constexpr int T = TS::T;
     constexpr int TN = TS::N;
     constexpr int SIDE = TS::SIDE;
-    __shared__ float4 tv[TN];      // grid velocity window
-    __shared__ float tm[4][TN];    // next-substep momentum / mass window
+    constexpr int MN = SCAT == 0 ? TS::MN : 1;
+    __shared__ float4 tv[TS::VN];  // grid velocity window
+    __shared__ float tm[4][MN];    // next-substep momentum / mass window (SCAT 0)
     __shared__ unsigned touched;   // 3^D neighbour-block bits
-
     __shared__ int s_chunk;
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.epoch, 1);
+
+    if (A.bump_epoch && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.epoch, 1);
     const int nch = *A.n_chunks;
     // persistent CTAs take chunks from a global cursor (chunk sizes vary)
     for (;;) {
@@ -249,16 +307,19 @@ __global__ void __launch_bounds__(kChunk, 2) k_g2p2g(ParticleBuf pb, FusedArgs A
         o[1] = (int)((lb / sc.nb[0]) % sc.nb[1]) * SIDE - 1;
         o[2] = (D == 3) ? (int)(lb / ((long long)sc.nb[0] * sc.nb[1])) * SIDE - 1 : 0;
         if (threadIdx.x == 0) touched = 0u;
-        for (int t = threadIdx.x; t < TN; t += blockDim.x) {
+        for (int t = threadIdx.x; t < TN; t += CHUNK) {
             const int tx = t % T, ty = (t / T) % T, tz = (D == 3) ? t / (T * T) : 0;
             const int ix = o[0] + tx, iy = o[1] + ty, iz = o[2] + tz;
             bool in = ix >= 0 && iy >= 0 && ix < sc.n[0] && iy < sc.n[1];
             if (D == 3) in = in && iz >= 0 && iz < sc.n[2];
-            tv[t] = in ? A.grid_vel[node_index<D>(sc, ix, iy, iz)] : make_float4(0.f, 0.f, 0.f, 0.f);
-            tm[0][t] = 0.f;
-            tm[1][t] = 0.f;
-            tm[2][t] = 0.f;
-            tm[3][t] = 0.f;
+            tv[tv_idx<D>(tx, ty, tz)] = in ? A.grid_vel[node_index<D>(sc, ix, iy, iz)] : make_float4(0.f, 0.f, 0.f, 0.f);
+            if (SCAT == 0) {
+                const int m = tm_idx<D>(tx, ty, tz);
+                tm[0][m] = 0.f;
+                tm[1][m] = 0.f;
+                tm[2][m] = 0.f;
+                tm[3][m] = 0.f;
+            }
         }
         __syncthreads();
 
@@ -275,47 +336,33 @@ __global__ void __launch_bounds__(kChunk, 2) k_g2p2g(ParticleBuf pb, FusedArgs A
             if (make_stencil<D>(x, sc, st, err)) {
                 // ---- G2P
                 G2PAcc<D> acc;
-                g2p_zero<D>(acc);
                 bool local = true;
 #pragma unroll
                 for (int a = 0; a < D; ++a) local = local && (st.base[a] - o[a] >= 0) && (st.base[a] - o[a] <= T - 3);
                 if (local) {
-                    const int l0 = st.base[0] - o[0], l1 = st.base[1] - o[1], l2 = D == 3 ? st.base[2] - o[2] : 0;
-#pragma unroll
-                    for (int ox = 0; ox < 3; ++ox)
-#pragma unroll
-                        for (int oy = 0; oy < 3; ++oy)
-#pragma unroll
-                            for (int oz = 0; oz < (D == 3 ? 3 : 1); ++oz) {
-                                const int off[3] = {ox, oy, oz};
-                                const int t = (l0 + ox) + T * ((l1 + oy) + (D == 3 ? T * (l2 + oz) : 0));
-                                g2p_node<D>(st, off, tv[t], sc.inv_h, acc);
-                            }
+                    const int b0 = st.base[0] - o[0], b1 = st.base[1] - o[1], b2 = D == 3 ? st.base[2] - o[2] : 0;
+                    g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) {
+                        return tv[tv_idx<D>(b0 + ox, b1 + oy, b2 + oz)];
+                    }, acc);
                 } else {
                     atomicAdd(A.fallback, 1u);
-#pragma unroll
-                    for (int ox = 0; ox < 3; ++ox)
-#pragma unroll
-                        for (int oy = 0; oy < 3; ++oy)
-#pragma unroll
-                            for (int oz = 0; oz < (D == 3 ? 3 : 1); ++oz) {
-                                const int off[3] = {ox, oy, oz};
-                                const long long gi = node_index<D>(sc, st.base[0] + ox, st.base[1] + oy,
-                                                                   D == 3 ? st.base[2] + oz : 0);
-                                g2p_node<D>(st, off, A.grid_vel[gi], sc.inv_h, acc);
-                            }
+                    g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) {
+                        return A.grid_vel[node_index<D>(sc, st.base[0] + ox, st.base[1] + oy,
+                                                        D == 3 ? st.base[2] + oz : 0)];
+                    }, acc);
                 }
                 // ---- particle update
                 float F[D * D], Cn[D * D], v[D];
-                float aux = S[P::AUX * cap + i];
-                if (g.type != WATER) {
+                float aux = 1.f;
+                if (MAT != JELLO) aux = S[P::AUX * cap + i];
+                if (MAT != WATER) {
 #pragma unroll
                     for (int k = 0; k < D * D; ++k) F[k] = S[(P::F + k) * cap + i];
                 } else {
 #pragma unroll
                     for (int k = 0; k < D * D; ++k) F[k] = (k % (D + 1) == 0) ? 1.f : 0.f;
                 }
-                err |= material_update<D>(acc, sc.dt, g, F, aux);
+                err |= material_update<D, MAT>(acc, sc.dt, g, F, aux);
                 const float c4 = 4.f * sc.inv_h;
 #pragma unroll
                 for (int a = 0; a < D; ++a) {
@@ -331,41 +378,42 @@ __global__ void __launch_bounds__(kChunk, 2) k_g2p2g(ParticleBuf pb, FusedArgs A
                 }
 #pragma unroll
                 for (int k = 0; k < D * D; ++k) S[(P::C + k) * cap + i] = Cn[k];
-                if (g.type != WATER) {
+                if (MAT != WATER) {
 #pragma unroll
                     for (int k = 0; k < D * D; ++k) S[(P::F + k) * cap + i] = F[k];
                 }
-                S[P::AUX * cap + i] = aux;
+                if (MAT != JELLO) S[P::AUX * cap + i] = aux;
 
                 // ---- stress + P2G of the next substep
                 Stencil<D> sn;
                 if (make_stencil<D>(x, sc, sn, err)) {
                     P2GSource<D> src;
-                    particle_stress_source<D>(v, Cn, F, aux, g, sc, src);
+                    particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc, src);
                     bool in_tile = true;
 #pragma unroll
                     for (int a = 0; a < D; ++a)
                         in_tile = in_tile && (sn.base[a] - o[a] >= 0) && (sn.base[a] - o[a] <= T - 3);
                     if (in_tile) {
                         const int l0 = sn.base[0] - o[0], l1 = sn.base[1] - o[1], l2 = D == 3 ? sn.base[2] - o[2] : 0;
-                        unsigned bits = 0u;
-#pragma unroll
-                        for (int ox = 0; ox < 3; ++ox)
-#pragma unroll
-                            for (int oy = 0; oy < 3; ++oy)
-#pragma unroll
-                                for (int oz = 0; oz < (D == 3 ? 3 : 1); ++oz) {
-                                    const int off[3] = {ox, oy, oz};
-                                    const float4 cc = p2g_node<D>(sn, src, off, sc.h, sc.inv_h);
-                                    const int t = (l0 + ox) + T * ((l1 + oy) + (D == 3 ? T * (l2 + oz) : 0));
-                                    atomicAdd(&tm[0][t], cc.x);
-                                    atomicAdd(&tm[1][t], cc.y);
-                                    if (D == 3) atomicAdd(&tm[2][t], cc.z);
-                                    atomicAdd(&tm[3][t], cc.w);
-                                }
+                        if (SCAT == 0) {
+                            p2g_scatter<D>(sn, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 cc) {
+                                const int m = tm_idx<D>(l0 + ox, l1 + oy, l2 + oz);
+                                atomicAdd(&tm[0][m], cc.x);
+                                atomicAdd(&tm[1][m], cc.y);
+                                if (D == 3) atomicAdd(&tm[2][m], cc.z);
+                                atomicAdd(&tm[3][m], cc.w);
+                            });
+                        } else {
+                            p2g_scatter<D>(sn, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 cc) {
+                                atomicAdd(&A.grid_mom[node_index<D>(sc, sn.base[0] + ox, sn.base[1] + oy,
+                                                                    D == 3 ? sn.base[2] + oz : 0)],
+                                          cc);
+                            });
+                        }
                         // neighbour-block slots covered by the stencil: the window starts
                         // one node below the home block, so local node l lies in block slot
                         // (l + SIDE - 1) / SIDE (0: home - 1, 1: home, 2: home + 1)
+                        unsigned bits = 0u;
 #pragma unroll
                         for (int cx = 0; cx < 2; ++cx)
 #pragma unroll
@@ -388,14 +436,16 @@ __global__ void __launch_bounds__(kChunk, 2) k_g2p2g(ParticleBuf pb, FusedArgs A
         }
         __syncthreads();
 
-        // ---- flush the momentum window
-        for (int t = threadIdx.x; t < TN; t += blockDim.x) {
-            const float m = tm[3][t];
-            const float mx = tm[0][t], my = tm[1][t], mz = tm[2][t];
-            if (m != 0.f || mx != 0.f || my != 0.f || mz != 0.f) {
+        // ---- flush the momentum window (SCAT 0) and mark touched blocks
+        if (SCAT == 0) {
+            for (int t = threadIdx.x; t < TN; t += CHUNK) {
                 const int tx = t % T, ty = (t / T) % T, tz = (D == 3) ? t / (T * T) : 0;
-                const int ix = o[0] + tx, iy = o[1] + ty, iz = o[2] + tz;
-                atomicAdd(&A.grid_mom[node_index<D>(sc, ix, iy, iz)], make_float4(mx, my, mz, m));
+                const int m = tm_idx<D>(tx, ty, tz);
+                const float mm = tm[3][m];
+                const float mx = tm[0][m], my = tm[1][m], mz = tm[2][m];
+                if (mm != 0.f || mx != 0.f || my != 0.f || mz != 0.f)
+                    atomicAdd(&A.grid_mom[node_index<D>(sc, o[0] + tx, o[1] + ty, o[2] + tz)],
+                              make_float4(mx, my, mz, mm));
             }
         }
         if ((int)threadIdx.x < (D == 3 ? 27 : 9) && ((touched >> threadIdx.x) & 1u)) {

@@ -48,19 +48,9 @@ __global__ void __launch_bounds__(128) k_p2g_direct(ParticleBuf pb, long long n,
     }
     P2GSource<D> src;
     particle_stress_source<D>(v, C, F, aux, g, sc, src);
-    const float h = sc.h, inv_h = sc.inv_h;
-#pragma unroll
-    for (int ox = 0; ox < 3; ++ox)
-#pragma unroll
-        for (int oy = 0; oy < 3; ++oy)
-#pragma unroll
-            for (int oz = 0; oz < (D == 3 ? 3 : 1); ++oz) {
-                const int o[3] = {ox, oy, oz};
-                const float4 c = p2g_node<D>(st, src, o, h, inv_h);
-                const long long gi = node_index<D>(sc, st.base[0] + ox, st.base[1] + oy,
-                                                   D == 3 ? st.base[2] + oz : 0);
-                atomicAdd(&grid[gi], c);
-            }
+    p2g_scatter<D>(st, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 c) {
+        atomicAdd(&grid[node_index<D>(sc, st.base[0] + ox, st.base[1] + oy, D == 3 ? st.base[2] + oz : 0)], c);
+    });
 }
 
 // Dense grid update over every node of every scene (VelUpdate,
@@ -109,19 +99,10 @@ __global__ void __launch_bounds__(128) k_g2p_direct(ParticleBuf pb, long long n,
         return;
     }
     G2PAcc<D> acc;
-    g2p_zero<D>(acc);
     const float inv_h = sc.inv_h;
-#pragma unroll
-    for (int ox = 0; ox < 3; ++ox)
-#pragma unroll
-        for (int oy = 0; oy < 3; ++oy)
-#pragma unroll
-            for (int oz = 0; oz < (D == 3 ? 3 : 1); ++oz) {
-                const int o[3] = {ox, oy, oz};
-                const long long gi = node_index<D>(sc, st.base[0] + ox, st.base[1] + oy,
-                                                   D == 3 ? st.base[2] + oz : 0);
-                g2p_node<D>(st, o, __ldg(&grid[gi]), inv_h, acc);
-            }
+    g2p_gather<D>(st, inv_h, [&](int ox, int oy, int oz) {
+        return __ldg(&grid[node_index<D>(sc, st.base[0] + ox, st.base[1] + oy, D == 3 ? st.base[2] + oz : 0)]);
+    }, acc);
     float F[D * D], aux = s[P::AUX * cap + i];
     if (g.type != WATER) {
 #pragma unroll

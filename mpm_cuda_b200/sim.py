@@ -90,7 +90,7 @@ class Simulation:
 
     def __init__(self, scenes: Sequence[Scene], p2g_mode: int = L.P2G_ATOMIC,
                  stress_mode: int = L.STRESS_PLAIN, use_graph: bool = True, device: int = 0,
-                 rebin_interval: int = 0):
+                 rebin_interval: int = 0, kernel_config: int = -1):
         lib = L.load()
         self.scenes = list(scenes)
         self.dim = self.scenes[0].dim
@@ -134,6 +134,7 @@ class Simulation:
         lib.mpm_default_options(C.byref(opt))
         opt.p2g_mode, opt.stress_mode, opt.use_graph, opt.device = p2g_mode, stress_mode, int(use_graph), device
         opt.rebin_interval = rebin_interval
+        opt.kernel_config = kernel_config
         h = C.c_void_p()
         L.check(lib.mpm_create(sdescs, len(self.scenes), C.byref(opt), C.byref(h)))
         self._h = h
@@ -241,6 +242,20 @@ class Simulation:
         n = C.c_int64()
         self._check(self._lib.mpm_count_active_nodes(self._h, scene, C.byref(n)))
         return n.value
+
+    def kernel_config(self) -> int:
+        c = C.c_int()
+        self._check(self._lib.mpm_get_kernel_config(self._h, C.byref(c)))
+        return c.value
+
+    def set_kernel_config(self, config: int):
+        self._check(self._lib.mpm_set_kernel_config(self._h, config))
+
+    def autotune(self, n_substeps: int = 8):
+        """(chosen configuration, ms per substep); does not advance the state."""
+        c, ms = C.c_int(), C.c_float()
+        self._check(self._lib.mpm_autotune(self._h, n_substeps, C.byref(c), C.byref(ms)))
+        return c.value, ms.value
 
     def bin_stats(self):
         """(fallback gathers/scatters served from global memory, re-binnings)."""

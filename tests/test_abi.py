@@ -38,7 +38,7 @@ def test_struct_sizes_match_header_layout():
     # natural alignment of the C structs in include/mpm_b200.h
     assert C.sizeof(L.MaterialDesc) == 8 + 8 * 8
     assert C.sizeof(L.GroupDesc) == 72 + 16 + 8 + 16 + 24 + 24
-    assert C.sizeof(L.Options) == 24
+    assert C.sizeof(L.Options) == 28
 
 
 def _mk(**kw):
@@ -81,6 +81,20 @@ def test_create_rejects_mixed_dims():
     with pytest.raises(L.MPMError) as e:
         Simulation([S.c0_jello2d(), S.c1_jello3d(n_grid=32, edge=0.2)])
     assert "same dim" in str(e.value)
+
+
+def test_kernel_config_table():
+    lib = L.load()
+    n = lib.mpm_num_kernel_configs()
+    assert n >= 2
+    seen = set()
+    for i in range(n):
+        ch, mb = C.c_int(), C.c_int()
+        assert lib.mpm_kernel_config_info(i, C.byref(ch), C.byref(mb)) == L.OK
+        assert ch.value in (64, 128, 256) and ch.value * mb.value <= 2048
+        seen.add((i, ch.value, mb.value))
+    assert len(seen) == n
+    assert lib.mpm_kernel_config_info(n, None, None) == L.ERR_INVALID
 
 
 def test_null_handle_calls_fail_cleanly():
