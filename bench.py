@@ -165,6 +165,8 @@ def cpu_baseline(scene, budget_s: float = 12.0):
 # ----------------------------------------------------------------- our arm
 
 def run_ours(args, rank, world, local_rank, dist):
+    import ctypes as C
+
     import torch
     from mpm_cuda_b200.sim import Simulation
 
@@ -173,7 +175,10 @@ def run_ours(args, rank, world, local_rank, dist):
     n_part = sum(s.n_particles for s in scenes)
     from mpm_cuda_b200 import _lib as L
     mode = {"binned": L.P2G_ATOMIC, "direct": L.P2G_DIRECT}[args.mode]
-    sim = Simulation(scenes, device=local_rank, p2g_mode=mode)
+    sim = Simulation(scenes, device=local_rank, p2g_mode=mode, kernel_config=args.kernel_config)
+    kcfg = sim.kernel_config()
+    chunk, min_ctas = C.c_int(), C.c_int()
+    L.load().mpm_kernel_config_info(kcfg, C.byref(chunk), C.byref(min_ctas))
     stream = torch.cuda.ExternalStream(sim.stream_ptr(), device=local_rank)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
 
@@ -219,7 +224,7 @@ def run_ours(args, rank, world, local_rank, dist):
         stage_names = ["rebin", "grid_update", "g2p2g"]
         alg = {"rebin": n_part * 2 * sp, "grid_update": active_nodes * 32,
                "g2p2g": n_part * 2 * sp + active_nodes * 32}
-        launches_per_step = 4  # grid update, fused kernel, 2 memset nodes
+        launches_per_step = 2  # grid update + one fused kernel per material present
     else:
         stage_names = ["p2g", "grid_update", "g2p"]
         alg = {"p2g": n_part * sp + active_nodes * 16, "grid_update": active_nodes * 32,
@@ -265,9 +270,12 @@ def run_ours(args, rank, world, local_rank, dist):
             "config": {"workload": desc, "particles_per_gpu": n_part, "particles_total": int(total_particles),
                        "active_nodes": active_nodes, "stress": "plain (SVD)", "path": args.mode,
                        "tile_fallbacks": fallbacks, "rebins": rebins,
+                       "kernel_config": {"index": kcfg, "chunk": chunk.value, "min_ctas_per_sm": min_ctas.value,
+                                         "chosen_by": "autotuner" if args.kernel_config < 0 else "flag"},
                        "l2": "flushed between substeps (256 MB write, outside the timed events)",
                        "parallelism": f"replicas x{world}" if args.workload != "c4" else f"scenes split over {world}"},
-            "roofline": roofline, "e2e": e2e, "gpu_launches": launches_per_step * args.steps + 6 * rebins,
+            "roofline": roofline, "e2e": e2e,
+            "gpu_launches": launches_per_step * args.steps + 10 * (args.steps // 16 + 1),
             "clocks": clocks}
     return line, scenes
 
@@ -319,6 +327,7 @@ def main():
     ap.add_argument("--workload", default="c1", choices=["c0", "c1", "c2", "c3", "c3big", "c4"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="binned", choices=["binned", "direct"])
+    ap.add_argument("--kernel-config", type=int, default=-1, help="fused-kernel configuration; -1 = autotune")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
