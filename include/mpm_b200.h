@@ -245,6 +245,27 @@ int mpm_autotune(mpm_handle *h, int n_substeps, int *chosen, float *ms_per_subst
  * memory) since creation; *rebins counts re-binnings. */
 int mpm_get_bin_stats(mpm_handle *h, int64_t *fallbacks, int64_t *rebins);
 
+/* Substeps without any device allocation, for callers that cannot allocate:
+ * code running while the application captures a CUDA graph, plug-in hosts
+ * with a fixed device memory budget, loops that forbid allocator calls after
+ * start-up.  No counterpart in the reference (its step() uses grids that its
+ * constructor allocated).
+ * Runs n_substeps of ONE scene with exactly one particle group (material,
+ * p_mass, p_vol from scene->groups[0]; its particle pointers are ignored)
+ * on the caller's stream.  `state` is caller-owned device memory in the
+ * handle's plane layout: x[dim], v[dim], C[dim*dim], F[dim*dim], aux, each
+ * plane `plane_stride` floats after the previous one; it is updated in place.
+ * The grid lives in a scratch area compiled into the library (8 MiB + 256 B
+ * per GPU, held until process exit) that fits at most 262,144 grid nodes
+ * counted in whole 64-node blocks (64^3 in 3D, 512^2 in 2D); larger grids are
+ * rejected with MPM_ERR_INVALID.  Every call shares that scratch, so calls
+ * whose work overlaps on the GPU race.  The first call on a device looks up the
+ * scratch address with that device current; make it before any stream
+ * capture begins.  Waits for the stream and returns MPM_ERR_SIM if the device
+ * error word is set.  Calls no cudaMalloc, cudaFree or allocating routine. */
+int mpm_step_noalloc(const mpm_scene_desc *scene, float *state, int64_t plane_stride,
+                     int64_t n_particles, int n_substeps, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

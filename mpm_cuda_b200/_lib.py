@@ -80,6 +80,7 @@ EXPORTS = {
     "mpm_get_kernel_config": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "mpm_set_kernel_config": (C.c_int, [C.c_void_p, C.c_int]),
     "mpm_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
+    "mpm_step_noalloc": (C.c_int, [C.POINTER(SceneDesc), C.c_void_p, C.c_int64, C.c_int64, C.c_int, C.c_void_p]),
 }
 
 _lib = None

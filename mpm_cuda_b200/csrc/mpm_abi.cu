@@ -26,6 +26,11 @@ thread_local std::string g_thread_error;
 
 using mpm::Engine;
 
+namespace mpm {
+// error text of calls that have no handle (read back by mpm_last_error(NULL))
+void set_thread_error(const char* msg) { g_thread_error = msg ? msg : ""; }
+}  // namespace mpm
+
 struct mpm_handle {
     Engine eng;
 };

@@ -85,18 +85,13 @@ def _f32(a, shape=None):
     return a
 
 
-class Simulation:
-    """One C-ABI handle over a list of scenes (all of the same dimension)."""
-
-    def __init__(self, scenes: Sequence[Scene], p2g_mode: int = L.P2G_ATOMIC,
-                 stress_mode: int = L.STRESS_PLAIN, use_graph: bool = True, device: int = 0,
-                 rebin_interval: int = 0, kernel_config: int = -1):
-        lib = L.load()
-        self.scenes = list(scenes)
-        self.dim = self.scenes[0].dim
-        keep = []
-        sdescs = (L.SceneDesc * len(self.scenes))()
-        for si, s in enumerate(self.scenes):
+def scene_descs(scenes: Sequence[Scene]):
+    """C descriptors (mpm_scene_desc[]) of the scenes, plus the list of
+    Python objects that must stay alive while the descriptors are used."""
+    keep = []
+    sdescs = (L.SceneDesc * len(scenes))()
+    for si, s in enumerate(scenes):
+        if True:
             gdescs = (L.GroupDesc * max(1, len(s.groups)))()
             keep.append(gdescs)
             for gi, g in enumerate(s.groups):
@@ -130,6 +125,19 @@ class Simulation:
             sd.mass_eps = s.mass_eps
             sd.n_groups = len(s.groups)
             sd.groups = gdescs
+    return sdescs, keep
+
+
+class Simulation:
+    """One C-ABI handle over a list of scenes (all of the same dimension)."""
+
+    def __init__(self, scenes: Sequence[Scene], p2g_mode: int = L.P2G_ATOMIC,
+                 stress_mode: int = L.STRESS_PLAIN, use_graph: bool = True, device: int = 0,
+                 rebin_interval: int = 0, kernel_config: int = -1):
+        lib = L.load()
+        self.scenes = list(scenes)
+        self.dim = self.scenes[0].dim
+        sdescs, keep = scene_descs(self.scenes)
         opt = L.Options()
         lib.mpm_default_options(C.byref(opt))
         opt.p2g_mode, opt.stress_mode, opt.use_graph, opt.device = p2g_mode, stress_mode, int(use_graph), device
