@@ -1,0 +1,376 @@
+// mpm_simulator.hpp -- the reference simulator's C++ interface over the C ABI.
+//
+// A header-only stand-in for the reference's MPMSimulator class
+// (src/simulator/MPMSimulator.cuh:66-102), its ObjInitInfo (:19-27), Material /
+// MaterialType (src/simulator/material/Elasiticity.cuh:10-45) and OutputBego
+// (src/utilities/FilesIO.h:10), with the same names and signatures, so that
+// the reference's main() (src/main.cpp:161-221) compiles against it.  Every
+// call forwards to include/mpm_b200.h; errors throw std::runtime_error (the
+// reference calls exit(1)).
+//
+// Seeding follows MPMSimulator.cpp:198-267: the object's model matrix is
+// translate * scale * rotate (model.cpp:202-207), its world bounding box must
+// lie inside the grid, and every grid cell of that box gets `ppc` uniformly
+// jittered samples kept when they fall inside the object.  `objPath` is
+//   "builtin:cube"      the cube [-0.5, 0.5]^3
+//   "builtin:sphere"    the ball of radius 0.5 at the origin
+//   "builtin:cylinder"  radius 0.5, height 1 along y, centred at the origin
+//   anything else       a Wavefront .obj file (v / f records), closed mesh,
+//                       inside test by ray-crossing parity
+// Differences from the reference: particle volume is h^3 / ppc (the reference
+// assigns h^3, MPMSimulator.cpp:252,263; set Options::reference_volume to
+// reproduce it); the random jitter comes from a seeded std::mt19937 instead of
+// rand(); positions are float on the device.
+#pragma once
+
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <fstream>
+#include <random>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "mpm_b200.h"
+
+// Elasiticity.cuh:10-11 (same enumerator values)
+enum MaterialType { JELLO = MPM_JELLO, SNOW = MPM_SNOW, WATER = MPM_WATER, SAND = MPM_SAND };
+
+// Elasiticity.cuh:19-45.  The constants the reference hard-codes in its
+// kernels are public members with the reference's values as defaults.
+class Material {
+   private:
+    double mYoungsModulus;
+    double mPoissonRatio;
+
+   public:
+    double mLambda;
+    double mMu;
+    double mDensity;
+    MaterialType mType;
+    double mXi = 10.0;       // snow hardening (MPMCUDA.cu:344)
+    double mThetaC = 8e-2;   // snow clamp below 1 (MPMCUDA.cu:658-660)
+    double mThetaS = 2e-2;   // snow clamp above 1
+    double mBulkK = 2.51;    // water pressure scale (MPMCUDA.cu:353)
+    double mGamma = 7.0;     // water exponent
+
+    Material() : mYoungsModulus(0.0), mPoissonRatio(0.0), mLambda(0.0), mMu(0.0), mDensity(0.0), mType(JELLO) {}
+
+    Material(double iYM, double iPR, double iDensity, MaterialType iType) : mType(iType) {
+        mYoungsModulus = iYM;
+        mPoissonRatio = iPR;
+        if (mYoungsModulus < 0) throw std::invalid_argument("Youngs Modulus is out of range.");
+        if (mPoissonRatio < 0 || mPoissonRatio > 0.5) throw std::invalid_argument("Poison Ratio is out of range.");
+        mMu = mYoungsModulus / (2 * (1 + mPoissonRatio));
+        mLambda = mYoungsModulus * mPoissonRatio / ((1 + mPoissonRatio) * (1 - 2 * mPoissonRatio));
+        mDensity = iDensity;
+    }
+    double youngsModulus() const { return mYoungsModulus; }
+    double poissonRatio() const { return mPoissonRatio; }
+};
+
+namespace mpm_shim {
+
+// float3 that also accepts glm::vec3 (anything indexable by [0..2])
+struct vec3 {
+    float x = 0.f, y = 0.f, z = 0.f;
+    vec3() = default;
+    vec3(float s) : x(s), y(s), z(s) {}
+    vec3(float a, float b, float c) : x(a), y(b), z(c) {}
+    template <class V, class = decltype(std::declval<const V&>()[0])>
+    vec3(const V& v) : x((float)v[0]), y((float)v[1]), z((float)v[2]) {}
+    float operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+};
+
+struct Mat3 {
+    double m[9];
+};
+
+// rotation by `deg` degrees about the (normalised) axis, Rodrigues' formula
+inline Mat3 rotation(double deg, vec3 axis) {
+    const double pi = 3.14159265358979323846;
+    double ax = axis.x, ay = axis.y, az = axis.z;
+    const double n = std::sqrt(ax * ax + ay * ay + az * az);
+    Mat3 r{{1, 0, 0, 0, 1, 0, 0, 0, 1}};
+    if (n == 0.0 || deg == 0.0) return r;
+    ax /= n;
+    ay /= n;
+    az /= n;
+    const double a = deg * pi / 180.0, c = std::cos(a), s = std::sin(a), t = 1.0 - c;
+    r.m[0] = t * ax * ax + c;      r.m[1] = t * ax * ay - s * az; r.m[2] = t * ax * az + s * ay;
+    r.m[3] = t * ax * ay + s * az; r.m[4] = t * ay * ay + c;      r.m[5] = t * ay * az - s * ax;
+    r.m[6] = t * ax * az - s * ay; r.m[7] = t * ay * az + s * ax; r.m[8] = t * az * az + c;
+    return r;
+}
+
+// closed triangle mesh with a ray-crossing inside test
+struct Mesh {
+    std::vector<double> v;     // xyz
+    std::vector<int> tri;      // 3 indices per triangle
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+
+    static Mesh load_obj(const std::string& path) {
+        std::ifstream f(path);
+        if (!f) throw std::runtime_error("cannot open " + path);
+        Mesh m;
+        std::string line;
+        while (std::getline(f, line)) {
+            std::istringstream ss(line);
+            std::string tag;
+            ss >> tag;
+            if (tag == "v") {
+                double a, b, c;
+                ss >> a >> b >> c;
+                m.v.insert(m.v.end(), {a, b, c});
+            } else if (tag == "f") {
+                std::vector<int> idx;
+                std::string tok;
+                while (ss >> tok) {
+                    int k = std::stoi(tok.substr(0, tok.find('/')));
+                    idx.push_back(k > 0 ? k - 1 : (int)(m.v.size() / 3) + k);
+                }
+                for (size_t j = 1; j + 1 < idx.size(); ++j) m.tri.insert(m.tri.end(), {idx[0], idx[j], idx[j + 1]});
+            }
+        }
+        if (m.tri.empty()) throw std::runtime_error(path + ": no faces");
+        for (size_t i = 0; i < m.v.size(); i += 3)
+            for (int a = 0; a < 3; ++a) {
+                m.lo[a] = std::min(m.lo[a], m.v[i + a]);
+                m.hi[a] = std::max(m.hi[a], m.v[i + a]);
+            }
+        return m;
+    }
+
+    // parity of crossings of a ray from p along a fixed skew direction
+    // (Moller-Trumbore ray/triangle test)
+    bool inside(const double* p) const {
+        const double d[3] = {0.8729436, 0.3961478, 0.2846573};
+        int hits = 0;
+        for (size_t t = 0; t < tri.size(); t += 3) {
+            const double* a = &v[3 * tri[t]];
+            const double* b = &v[3 * tri[t + 1]];
+            const double* c = &v[3 * tri[t + 2]];
+            const double e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+            const double e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+            const double q[3] = {d[1] * e2[2] - d[2] * e2[1], d[2] * e2[0] - d[0] * e2[2], d[0] * e2[1] - d[1] * e2[0]};
+            const double det = e1[0] * q[0] + e1[1] * q[1] + e1[2] * q[2];
+            if (std::fabs(det) < 1e-300) continue;
+            const double inv = 1.0 / det;
+            const double s[3] = {p[0] - a[0], p[1] - a[1], p[2] - a[2]};
+            const double u = (s[0] * q[0] + s[1] * q[1] + s[2] * q[2]) * inv;
+            if (u < 0.0 || u > 1.0) continue;
+            const double r[3] = {s[1] * e1[2] - s[2] * e1[1], s[2] * e1[0] - s[0] * e1[2], s[0] * e1[1] - s[1] * e1[0]};
+            const double w = (d[0] * r[0] + d[1] * r[1] + d[2] * r[2]) * inv;
+            if (w < 0.0 || u + w > 1.0) continue;
+            if ((e2[0] * r[0] + e2[1] * r[1] + e2[2] * r[2]) * inv > 0.0) ++hits;
+        }
+        return (hits & 1) != 0;
+    }
+};
+
+}  // namespace mpm_shim
+
+// MPMSimulator.cuh:19-27
+struct ObjInitInfo {
+    std::array<double, 3> initVel{};
+    mpm_shim::vec3 initTranslation;
+    mpm_shim::vec3 initRotationAxis{0.f, 1.f, 0.f};
+    mpm_shim::vec3 initScale{1.f};
+    float initRotationDegree = 0.f;
+    std::string objPath;
+    Material mMaterial;
+};
+
+// MPMSimulator.cuh:66-102
+class MPMSimulator {
+   public:
+    struct Options {
+        // wall band of the reference's VelUpdate: components zeroed at nodes with
+        // index <= 10 or >= n - 10 (MPMCUDA.cu:845-850, 467-469)
+        int bc_type = MPM_BC_SLIP;
+        int bc_lo = 11, bc_hi = 10;
+        double gravity_y = -9.8;           // MPMSimulator.cpp:186
+        double mass_eps = 2.220446049250313e-16;  // MPMCUDA.cu:444
+        bool reference_volume = false;     // particle volume h^3 as the reference seeds
+        unsigned seed = 1234;              // jitter generator
+        int p2g_mode = MPM_P2G_ATOMIC;
+        int device = 0;
+    };
+
+    // the grid fields of the reference's Grid (MPMSimulator.cuh:54-64) that its
+    // viewer reads (main.cpp:170-175); the grid arrays live on the device
+    struct Grid {
+        double h = 0.0;
+        unsigned int nodeNumDimX = 0, nodeNumDimY = 0, nodeNumDimZ = 0;
+        std::array<double, 3> originCorner{{0.0, 0.0, 0.0}};
+    };
+
+    double adp_dt;
+    double current_time;
+    int current_frame;
+    Grid mGrid{};
+
+    MPMSimulator(double gap, double dt, unsigned int nodeNumDimX, unsigned int nodeNumDimY,
+                 unsigned int nodeNumDimZ, unsigned int particleNumPerCell,
+                 std::vector<ObjInitInfo>& objInitInfoVec)
+        : MPMSimulator(gap, dt, nodeNumDimX, nodeNumDimY, nodeNumDimZ, particleNumPerCell, objInitInfoVec,
+                       Options()) {}
+
+    MPMSimulator(double gap, double dt, unsigned int nx, unsigned int ny, unsigned int nz, unsigned int ppc,
+                 std::vector<ObjInitInfo>& objs, const Options& opt)
+        : adp_dt(dt), current_time(0.0), current_frame(0) {
+        mGrid.h = gap;
+        mGrid.nodeNumDimX = nx;
+        mGrid.nodeNumDimY = ny;
+        mGrid.nodeNumDimZ = nz;
+        std::mt19937 rng(opt.seed);
+        std::uniform_real_distribution<float> U(0.f, 1.f);
+        std::vector<std::vector<float>> pos(objs.size());
+        std::vector<mpm_group_desc> groups(objs.size());
+        const unsigned n[3] = {nx, ny, nz};
+        for (size_t k = 0; k < objs.size(); ++k) {
+            const ObjInitInfo& o = objs[k];
+            seed_object(o, gap, n, ppc, rng, U, pos[k]);
+            const Material& m = o.mMaterial;
+            mpm_group_desc& g = groups[k];
+            g = mpm_group_desc{};
+            g.material.type = m.mType;
+            g.material.E = m.youngsModulus();
+            g.material.nu = m.poissonRatio();
+            g.material.rho = m.mDensity;
+            g.material.xi = m.mXi;
+            g.material.theta_c = m.mThetaC;
+            g.material.theta_s = m.mThetaS;
+            g.material.bulk_k = m.mBulkK;
+            g.material.gamma = m.mGamma;
+            g.p_vol = opt.reference_volume ? gap * gap * gap : gap * gap * gap / ppc;
+            g.p_mass = m.mDensity * g.p_vol;
+            g.n = (int64_t)(pos[k].size() / 3);
+            g.x = pos[k].data();
+            for (int a = 0; a < 3; ++a) g.init_v[a] = o.initVel[a];
+        }
+        mpm_scene_desc sc{};
+        sc.dim = 3;
+        sc.n[0] = (int)nx;
+        sc.n[1] = (int)ny;
+        sc.n[2] = (int)nz;
+        sc.h = gap;
+        sc.dt = dt;
+        sc.gravity[1] = opt.gravity_y;
+        sc.bc_type = opt.bc_type;
+        sc.bc_lo = opt.bc_lo;
+        sc.bc_hi = opt.bc_hi;
+        sc.mass_eps = opt.mass_eps;
+        sc.n_groups = (int)groups.size();
+        sc.groups = groups.data();
+        mpm_options mo;
+        mpm_default_options(&mo);
+        mo.p2g_mode = opt.p2g_mode;
+        mo.device = opt.device;
+        check(mpm_create(&sc, 1, &mo, &h_), nullptr);
+    }
+
+    MPMSimulator(const MPMSimulator&) = delete;
+    MPMSimulator& operator=(const MPMSimulator&) = delete;
+
+    ~MPMSimulator() {
+        if (h_) mpm_destroy(h_);
+    }
+
+    // MPMCUDA.cu:793-925: one substep of every particle group
+    void step() {
+        check(mpm_step(h_, 1), h_);
+        ++current_frame;
+        current_time += adp_dt;
+    }
+
+    int totalParticlesNum() {
+        int64_t n = 0;
+        check(mpm_num_particles(h_, -1, &n), h_);
+        return (int)n;
+    }
+
+    // MPMSimulator.cpp:362-371: positions of every group, in group order
+    void getGLParticlesPos(std::vector<float>& oPosVec) {
+        oPosVec.resize((size_t)totalParticlesNum() * 3);
+        check(mpm_get_positions(h_, 0, oPosVec.data(), oPosVec.size()), h_);
+    }
+
+    mpm_handle* handle() { return h_; }
+
+   private:
+    mpm_handle* h_ = nullptr;
+
+    static void check(int rc, mpm_handle* h) {
+        if (rc == MPM_OK) return;
+        char buf[512];
+        mpm_last_error(h, buf, sizeof(buf));
+        throw std::runtime_error(std::string("mpm_b200: ") + buf);
+    }
+
+    static void seed_object(const ObjInitInfo& o, double gap, const unsigned* n, unsigned ppc, std::mt19937& rng,
+                            std::uniform_real_distribution<float>& U, std::vector<float>& out) {
+        using mpm_shim::Mesh;
+        const mpm_shim::Mat3 R = mpm_shim::rotation(o.initRotationDegree, o.initRotationAxis);
+        const double S[3] = {o.initScale.x, o.initScale.y, o.initScale.z};
+        const double T[3] = {o.initTranslation.x, o.initTranslation.y, o.initTranslation.z};
+        int shape = -1;  // 0 cube, 1 sphere, 2 cylinder, 3 mesh
+        Mesh mesh;
+        double llo[3] = {-0.5, -0.5, -0.5}, lhi[3] = {0.5, 0.5, 0.5};
+        if (o.objPath == "builtin:cube") shape = 0;
+        else if (o.objPath == "builtin:sphere") shape = 1;
+        else if (o.objPath == "builtin:cylinder") shape = 2;
+        else {
+            shape = 3;
+            mesh = Mesh::load_obj(o.objPath);
+            for (int a = 0; a < 3; ++a) {
+                llo[a] = mesh.lo[a];
+                lhi[a] = mesh.hi[a];
+            }
+        }
+        // world bounding box of the transformed local box (model.cpp:202-222)
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int c = 0; c < 8; ++c) {
+            const double p[3] = {(c & 1) ? lhi[0] : llo[0], (c & 2) ? lhi[1] : llo[1], (c & 4) ? lhi[2] : llo[2]};
+            for (int a = 0; a < 3; ++a) {
+                const double w = T[a] + S[a] * (R.m[a * 3] * p[0] + R.m[a * 3 + 1] * p[1] + R.m[a * 3 + 2] * p[2]);
+                lo[a] = std::min(lo[a], w);
+                hi[a] = std::max(hi[a], w);
+            }
+        }
+        for (int a = 0; a < 3; ++a) {
+            if (lo[a] < 0.0) throw std::runtime_error("ERROR: OBJ lower bound is smaller than grid's origin.");
+            if (hi[a] > (n[a] - 1) * gap) throw std::runtime_error("ERROR: OBJ upper bound is out of the grid.");
+        }
+        int i0[3], i1[3];
+        for (int a = 0; a < 3; ++a) {
+            i0[a] = (int)(lo[a] / gap);
+            i1[a] = (int)(hi[a] / gap) + 1;
+        }
+        for (int ix = i0[0]; ix < i1[0]; ++ix)
+            for (int iy = i0[1]; iy < i1[1]; ++iy)
+                for (int iz = i0[2]; iz < i1[2]; ++iz)
+                    for (unsigned ip = 0; ip < ppc; ++ip) {
+                        const float wp[3] = {(float)(ix * gap + U(rng) * gap), (float)(iy * gap + U(rng) * gap),
+                                             (float)(iz * gap + U(rng) * gap)};
+                        // local = R^T ((world - T) / S)
+                        double q[3], l[3];
+                        for (int a = 0; a < 3; ++a) q[a] = (wp[a] - T[a]) / S[a];
+                        for (int a = 0; a < 3; ++a) l[a] = R.m[a] * q[0] + R.m[3 + a] * q[1] + R.m[6 + a] * q[2];
+                        bool in;
+                        if (shape == 0) in = std::fabs(l[0]) <= 0.5 && std::fabs(l[1]) <= 0.5 && std::fabs(l[2]) <= 0.5;
+                        else if (shape == 1) in = l[0] * l[0] + l[1] * l[1] + l[2] * l[2] <= 0.25;
+                        else if (shape == 2) in = l[0] * l[0] + l[2] * l[2] <= 0.25 && std::fabs(l[1]) <= 0.5;
+                        else in = mesh.inside(l);
+                        if (in) out.insert(out.end(), {wp[0], wp[1], wp[2]});
+                    }
+    }
+};
+
+// FilesIO.h:10 -- writes positions (x y z per particle) as a .bgeo file
+inline void OutputBego(const std::string& fileNamePath, const std::vector<float>& outPosData) {
+    if (mpm_write_bgeo_positions(fileNamePath.c_str(), outPosData.data(), (int64_t)(outPosData.size() / 3)) != MPM_OK)
+        throw std::runtime_error("OutputBego: cannot write " + fileNamePath);
+}
