@@ -218,7 +218,7 @@ int mpm_last_error(mpm_handle *h, char *buf, size_t cap);
  * n_substeps).  out_ms[0..n_out) in stage order:
  *   MPM_P2G_ATOMIC:  rebin (one re-binning), grid_update, g2p2g
  *   MPM_P2G_DIRECT:  p2g, grid_update, g2p
- *   MPM_P2G_DETERMINISTIC: g2p, sort, p2g_gather, grid_update
+ *   MPM_P2G_DETERMINISTIC: grid_update, g2p, p2g (source + sort + gather)
  * *n_written receives the number of stages written. */
 int mpm_profile_stages(mpm_handle *h, int n_substeps, float *out_ms, int n_out,
                        int *n_written);

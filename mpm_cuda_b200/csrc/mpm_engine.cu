@@ -13,6 +13,7 @@
 #include <mutex>
 
 #include "mpm_kernels_binned.cuh"
+#include "mpm_kernels_det.cuh"
 #include "mpm_kernels_direct.cuh"
 
 namespace mpm {
@@ -32,6 +33,19 @@ __global__ void k_unpermute(const float* __restrict__ in, float* __restrict__ ou
     if (i >= n) return;
     const long long j = id[i];
     for (int p = 0; p < planes; ++p) out[p * cap + j] = in[p * cap + i];
+}
+
+// planes, group and creation index of every particle moved to its creation
+// index (afterwards id[j] == j)
+__global__ void k_canonicalize(const float* __restrict__ in, float* __restrict__ out, const uint16_t* __restrict__ gin,
+                               uint16_t* __restrict__ gout, const uint32_t* __restrict__ id, uint32_t* __restrict__ id_out,
+                               long long n, long long cap, int planes) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long j = id[i];
+    for (int p = 0; p < planes; ++p) out[p * cap + j] = in[p * cap + i];
+    gout[j] = gin[i];
+    id_out[j] = (uint32_t)j;
 }
 
 // out[i] = in[id[i]] for particles whose creation index lies in [lo, hi)
@@ -300,6 +314,12 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
         if ((rc = alloc((void**)&vals[p], cap * sizeof(unsigned), "sort values")) != MPM_OK) return rc;
     }
     if ((rc = alloc((void**)&cell_count, total_blocks * 64 * sizeof(int), "cell counts")) != MPM_OK) return rc;
+    if ((rc = alloc((void**)&cell_end, total_blocks * 64 * sizeof(int), "cell ends")) != MPM_OK) return rc;
+    {
+        const int src_planes = dim == 3 ? SrcPlanes<3>::COUNT : SrcPlanes<2>::COUNT;
+        if ((rc = alloc((void**)&det_src, (size_t)src_planes * cap * sizeof(float), "source records")) != MPM_OK)
+            return rc;
+    }
     if ((rc = alloc((void**)&seg_count, total_blocks * 4 * sizeof(int), "segment counts")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&seg_start, total_blocks * 4 * sizeof(int), "segment starts")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&blk_flag, total_blocks * sizeof(unsigned), "blk_flag")) != MPM_OK) return rc;
@@ -310,8 +330,15 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     if ((rc = alloc((void**)&chunks, kMats * list_cap * sizeof(Chunk), "chunks")) != MPM_OK) return rc;
     key_bits = 12;
     while (key_bits < 64 && (1LL << (key_bits - 12)) < total_blocks) ++key_bits;
+    det_key_bits = 1;
+    while (det_key_bits < 64 && (1LL << det_key_bits) <= total_blocks * 64) ++det_key_bits;
     cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp_bytes, keys[0], keys[1], vals[0], vals[1], (int)cap, 0,
                                     key_bits);
+    {
+        size_t det_bytes = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, det_bytes, keys[0], keys[1], vals[0], vals[1], (int)cap, 0, 64);
+        sort_tmp_bytes = std::max(sort_tmp_bytes, det_bytes);
+    }
     if ((rc = alloc(&sort_tmp, sort_tmp_bytes, "sort temp")) != MPM_OK) return rc;
     cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp_bytes, seg_count, seg_start, (int)(total_blocks * 4));
     if ((rc = alloc(&scan_tmp, scan_tmp_bytes, "scan temp")) != MPM_OK) return rc;
@@ -335,6 +362,7 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     if (e == cudaSuccess) e = cudaMemset(err_d, 0, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(blk_flag, 0, total_blocks * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(cell_count, 0, total_blocks * 64 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(cell_end, 0, total_blocks * 64 * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(seg_count, 0, total_blocks * 4 * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(blk_epoch, 0xff, total_blocks * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(counters, 0, CNT_N * sizeof(int));
@@ -504,7 +532,7 @@ void Engine::release() {
     }
     void* ptrs[] = {groups_d, scenes_d, grid_mom, grid_vel, err_d, keys[0], keys[1], vals[0], vals[1],
                     cell_count, seg_count, seg_start, sort_tmp, blk_flag, active, blk_epoch, counters, chunks,
-                    scan_tmp, pos_out};
+                    scan_tmp, pos_out, cell_end, det_src};
     for (void* p : ptrs) cudaFree(p);
     groups_d = nullptr;
     scenes_d = nullptr;
@@ -512,7 +540,8 @@ void Engine::release() {
     err_d = nullptr;
     keys[0] = keys[1] = nullptr;
     vals[0] = vals[1] = nullptr;
-    cell_count = seg_count = seg_start = nullptr;
+    cell_count = seg_count = seg_start = cell_end = nullptr;
+    det_src = nullptr;
     sort_tmp = nullptr;
     blk_flag = nullptr;
     active = blk_epoch = counters = nullptr;
@@ -594,6 +623,7 @@ void Engine::enqueue_rebin(int from) {
     note_launch("k_bin_reset");
     k_count_rebin<<<1, 1, 0, stream>>>(counters + CNT_REBINS);
     note_launch("k_count_rebin");
+    sorted_order = true;
 }
 
 FusedArgs Engine::fused_args(int mat, bool bump) {
@@ -648,6 +678,74 @@ void Engine::enqueue_fused_substep(int parity) {
     enqueue_g2p2g(parity);
 }
 
+// deterministic P2G of the current state into grid_mom (blocks marked active)
+void Engine::enqueue_det_p2g() {
+    const int n_scenes = (int)scenes_h.size();
+    if (n_particles > 0) {
+        if (dim == 3)
+            k_det_source<3><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(
+                buf(cur), n_particles, groups_d, scenes_d, det_src, cap, keys[0], vals[0], blk_flag, active,
+                counters + CNT_ACTIVE, err_d);
+        else
+            k_det_source<2><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(
+                buf(cur), n_particles, groups_d, scenes_d, det_src, cap, keys[0], vals[0], blk_flag, active,
+                counters + CNT_ACTIVE, err_d);
+        note_launch("k_det_source");
+        // the no-cell key is all ones: sort on every bit so it lands last
+        cub::DeviceRadixSort::SortPairs(sort_tmp, sort_tmp_bytes, keys[0], keys[1], vals[0], vals[1],
+                                        (int)n_particles, 0, 64, stream);
+        note_launch("cub::DeviceRadixSort::SortPairs");
+        k_det_ranges<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys[1], n_particles, cell_count, cell_end);
+        note_launch("k_det_ranges");
+    }
+    if (dim == 3)
+        k_det_gather<3><<<update_ctas, 256, 0, stream>>>(det_src, cap, vals[1], cell_count, cell_end, active,
+                                                         counters + CNT_ACTIVE, scenes_d, n_scenes, grid_mom);
+    else
+        k_det_gather<2><<<update_ctas, 256, 0, stream>>>(det_src, cap, vals[1], cell_count, cell_end, active,
+                                                         counters + CNT_ACTIVE, scenes_d, n_scenes, grid_mom);
+    note_launch("k_det_gather");
+    if (n_particles > 0) {
+        k_det_reset<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys[1], n_particles, cell_count, cell_end);
+        note_launch("k_det_reset");
+    }
+}
+
+// grid update of the pending P2G, G2P from it, deterministic P2G of the result
+void Engine::enqueue_det_substep() {
+    enqueue_grid_update();
+    const ParticleBuf pb = buf(cur);
+    const int bt = opt.block_threads > 0 ? opt.block_threads : 128;
+    if (n_particles > 0) {
+        if (dim == 3)
+            k_g2p_direct<3><<<grid_blocks(n_particles, bt), bt, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
+                                                                             grid_vel, err_d);
+        else
+            k_g2p_direct<2><<<grid_blocks(n_particles, bt), bt, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
+                                                                             grid_vel, err_d);
+        note_launch("k_g2p_direct");
+    }
+    // the epoch is bumped once per substep (the fused kernel does it in its path)
+    k_count_rebin<<<1, 1, 0, stream>>>(counters + CNT_EPOCH);
+    note_launch("epoch");
+    enqueue_det_p2g();
+}
+
+// moves the particles back to creation order (deterministic mode needs an
+// order that does not depend on atomics)
+int Engine::canonical_order() {
+    if (!sorted_order) return MPM_OK;
+    if (n_particles > 0) {
+        k_canonicalize<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(st[cur], st[1 - cur], gp[cur], gp[1 - cur],
+                                                                          ids[cur], ids[1 - cur], n_particles, cap,
+                                                                          n_planes);
+        note_launch("k_canonicalize");
+        cur = 1 - cur;
+    }
+    sorted_order = false;
+    return take_launch_error();
+}
+
 // makes grid_mom hold the P2G of the current state (binned path): sorts the
 // particles into fresh chunks and scatters them straight to global memory
 int Engine::prologue() {
@@ -655,6 +753,15 @@ int Engine::prologue() {
     MPM_CUDA_TRY(cudaMemsetAsync(grid_mom, 0, grid_bytes, stream), "prologue clear");
     MPM_CUDA_TRY(cudaMemsetAsync(blk_flag, 0, total_blocks * sizeof(unsigned), stream), "prologue flags");
     MPM_CUDA_TRY(cudaMemsetAsync(counters + CNT_ACTIVE, 0, sizeof(int), stream), "prologue counters");
+    if (deterministic()) {
+        int rc = canonical_order();
+        if (rc != MPM_OK) return rc;
+        enqueue_det_p2g();
+        rc = take_launch_error();
+        if (rc != MPM_OK) return rc;
+        grid_dirty = false;
+        return MPM_OK;
+    }
     enqueue_rebin(cur);
     cur = 1 - cur;
     steps_since_rebin = 0;
@@ -707,7 +814,7 @@ int Engine::step(int n) {
         return MPM_ERR_INVALID;
     }
     MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
-    if (!fused()) {
+    if (direct()) {
         if (grid_dirty) {
             MPM_CUDA_TRY(cudaMemsetAsync(grid_mom, 0, (size_t)total_blocks * 64 * sizeof(float4), stream),
                          "grid clear");
@@ -728,6 +835,35 @@ int Engine::step(int n) {
         } else {
             for (int i = 0; i < n; ++i) enqueue_direct_substep();
             MPM_CUDA_TRY(cudaGetLastError(), "kernel launch");
+        }
+    } else if (deterministic()) {
+        if (grid_dirty) {
+            int rc = prologue();
+            if (rc != MPM_OK) return rc;
+        }
+        if (opt.use_graph) {
+            if (!graphs[cur][0]) {
+                cudaGraph_t g = nullptr;
+                MPM_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture begin");
+                enqueue_det_substep();
+                cudaError_t e = cudaStreamEndCapture(stream, &g);
+                if (e != cudaSuccess) {
+                    take_launch_error();
+                    return cuda_fail(e, "capture end");
+                }
+                if (take_launch_error() != MPM_OK) {
+                    cudaGraphDestroy(g);
+                    return MPM_ERR_CUDA;
+                }
+                e = cudaGraphInstantiate(&graphs[cur][0], g, 0);
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
+            }
+            for (int i = 0; i < n; ++i) MPM_CUDA_TRY(cudaGraphLaunch(graphs[cur][0], stream), "graph launch");
+        } else {
+            for (int i = 0; i < n; ++i) enqueue_det_substep();
+            const int lrc = take_launch_error();
+            if (lrc != MPM_OK) return lrc;
         }
     } else {
         if (grid_dirty) {
@@ -877,7 +1013,7 @@ int Engine::get_grid(int scene, float* mass, float* vel) {
     std::vector<float4> blk((size_t)sc.n_nodes);
     MPM_CUDA_TRY(cudaMemcpy(blk.data(), grid_vel + sc.node_off, sc.n_nodes * sizeof(float4), cudaMemcpyDeviceToHost),
                  "grid download");
-    if (fused()) {
+    if (!direct()) {
         // blocks not stamped by the last grid update hold stale values
         std::vector<int> ep((size_t)sc.n_blocks);
         int cnt[CNT_N];
@@ -972,6 +1108,34 @@ int Engine::profile_stages(int n, float* out_ms, int n_out, int* n_written) {
             acc[1] += a;
             acc[2] += b;
             ++steps_since_rebin;
+        }
+    } else if (deterministic()) {
+        if (grid_dirty) {
+            int rc = prologue();
+            if (rc != MPM_OK) return rc;
+        }
+        const ParticleBuf pb = buf(cur);
+        for (int it = 0; it < n; ++it) {
+            cudaEventRecord(ev[0], stream);
+            enqueue_grid_update();
+            cudaEventRecord(ev[1], stream);
+            if (dim == 3)
+                k_g2p_direct<3><<<grid_blocks(n_particles, bt), bt, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
+                                                                                 grid_vel, err_d);
+            else
+                k_g2p_direct<2><<<grid_blocks(n_particles, bt), bt, 0, stream>>>(pb, n_particles, groups_d, scenes_d,
+                                                                                 grid_vel, err_d);
+            note_launch("k_g2p_direct");
+            k_count_rebin<<<1, 1, 0, stream>>>(counters + CNT_EPOCH);
+            cudaEventRecord(ev[2], stream);
+            enqueue_det_p2g();
+            cudaEventRecord(ev[3], stream);
+            cudaEventSynchronize(ev[3]);
+            for (int st_i = 0; st_i < 3; ++st_i) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ev[st_i], ev[st_i + 1]);
+                acc[st_i] += ms;
+            }
         }
     } else {
         const ParticleBuf pb = buf(cur);

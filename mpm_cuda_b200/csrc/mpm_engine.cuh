@@ -48,6 +48,10 @@ struct Engine {
     unsigned long long* keys[2] = {nullptr, nullptr};  // radix sort keys in / out
     unsigned* vals[2] = {nullptr, nullptr};            // particle index in / sorted
     int* cell_count = nullptr;  // per node of every block: particles whose base is that node
+    int* cell_end = nullptr;    // deterministic mode: end of each base node's records
+    float* det_src = nullptr;   // deterministic mode: P2G source records
+    int det_key_bits = 64;
+    bool sorted_order = false;  // particles permuted away from creation order
     int* seg_count = nullptr;   // per (block, material)
     int* seg_start = nullptr;
     void* sort_tmp = nullptr;
@@ -112,6 +116,11 @@ struct Engine {
     void drop_graphs();
     int unpermute_to_alt();
     bool fused() const { return opt.p2g_mode == MPM_P2G_ATOMIC; }
+    bool deterministic() const { return opt.p2g_mode == MPM_P2G_DETERMINISTIC; }
+    bool direct() const { return opt.p2g_mode == MPM_P2G_DIRECT; }
+    void enqueue_det_p2g();
+    void enqueue_det_substep();
+    int canonical_order();
 };
 
 }  // namespace mpm

@@ -27,8 +27,8 @@ def blob_scene(d, name, bc=L.BC_SLIP, seed=3, n_grid=32, h=1.0 / 32, ppc=2, radi
                  gravity=(0.0, -9.8, 0.0)[:d] if d == 3 else (0.0, -9.8), **kw)
 
 
-MODES = [L.P2G_ATOMIC, L.P2G_DIRECT]
-MODE_IDS = ["binned", "direct"]
+MODES = [L.P2G_ATOMIC, L.P2G_DIRECT, L.P2G_DETERMINISTIC]
+MODE_IDS = ["binned", "direct", "deterministic"]
 
 
 @pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
@@ -280,3 +280,44 @@ def test_set_state_mid_run_binned(gpu):
     orc = oracle_for(sc2)
     assert orc.step(2) == 0
     compare(got, orc.state(), {"x": 5e-6, "v": 5e-4, "C": 5e-4, "F": 3e-5, "aux": 3e-5})
+
+
+def _mixed_scene(seed):
+    a = blob_scene(3, "jello", seed=seed)
+    for name, shift in (("snow", 4), ("water", -4)):
+        b = blob_scene(3, name, seed=seed + shift)
+        for g in b.groups:
+            g.x[:, 1] += np.float32(shift * a.h)
+        a.groups += b.groups
+    return a
+
+
+def test_deterministic_mode_is_bitwise_reproducible(gpu):
+    results = []
+    for _ in range(2):
+        with Simulation([_mixed_scene(110)], p2g_mode=L.P2G_DETERMINISTIC) as sim:
+            sim.step(12)
+            results.append((sim.get_state(0), sim.get_grid(0)))
+    (s0, g0), (s1, g1) = results
+    for k in ("x", "v", "C", "F", "aux"):
+        assert np.array_equal(s0[k], s1[k]), k
+    assert np.array_equal(g0[0], g1[0]) and np.array_equal(g0[1], g1[1])
+
+
+def test_deterministic_after_binned_steps_is_reproducible(gpu):
+    # binned steps permute the particles (atomically ranked sort keys); the
+    # deterministic mode first restores creation order, so two handles whose
+    # storage orders differ agree bitwise once they hold the same state
+    with Simulation([_mixed_scene(120)]) as sim:
+        sim.step(3)
+        st = sim.get_state(0)
+    outs = []
+    for _ in range(2):
+        with Simulation([_mixed_scene(120)], rebin_interval=2) as sim:
+            sim.step(5)
+            sim.set_p2g_mode(L.P2G_DETERMINISTIC)
+            sim.set_state(0, x=st["x"], v=st["v"], C_=st["C"], F=st["F"], aux=st["aux"])
+            sim.step(6)
+            outs.append(sim.get_state(0))
+    for k in ("x", "v", "C", "F", "aux"):
+        assert np.array_equal(outs[0][k], outs[1][k]), k
