@@ -216,7 +216,8 @@ int mpm_last_error(mpm_handle *h, char *buf, size_t cap);
 /* Per-stage device time of one substep, measured with CUDA events on the
  * handle's stream and averaged over n_substeps (the handle advances by
  * n_substeps).  out_ms[0..n_out) in stage order:
- *   MPM_P2G_ATOMIC:  rebin (one re-binning), grid_update, g2p2g
+ *   MPM_P2G_ATOMIC:  rebin (time of one re-binning; they run every
+ *                    rebin_interval substeps as in mpm_step), grid_update, g2p2g
  *   MPM_P2G_DIRECT:  p2g, grid_update, g2p
  *   MPM_P2G_DETERMINISTIC: grid_update, g2p, p2g (source + sort + gather)
  * *n_written receives the number of stages written. */
@@ -265,6 +266,76 @@ int mpm_get_bin_stats(mpm_handle *h, int64_t *fallbacks, int64_t *rebins);
  * error word is set.  Calls no cudaMalloc, cudaFree or allocating routine. */
 int mpm_step_noalloc(const mpm_scene_desc *scene, float *state, int64_t plane_stride,
                      int64_t n_particles, int n_substeps, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Learned stress surrogate.  No counterpart in the reference, whose stress
+ * pass always takes an SVD (MPMCUDA.cu:87-134, 229-264).  A BF16 MLP
+ * 10 -> 64 -> 64 -> 9 (SiLU) predicts the residual of sqrt(F F^T) beyond its
+ * second-order series; the Kirchhoff stress of jello and of snow's elastic
+ * part follows from it without an SVD.  Training and inference run on the
+ * GPU's tensor cores; particles outside the training envelope, or whose error
+ * estimate is above skew_tol, take the SVD path.
+ * ---------------------------------------------------------------------- */
+typedef struct mpm_surrogate mpm_surrogate;
+
+typedef struct mpm_surrogate_train_options {
+    int64_t n_samples;       /* training samples generated from the seeds */
+    int epochs;              /* passes over the samples */
+    int batch;               /* mini-batch, a multiple of 128 */
+    float lr, lr_final;      /* Adam learning rate, cosine-decayed */
+    float sigma;             /* std of the singular-value perturbation */
+    float rotation_fraction; /* share of samples with a uniformly random rotation */
+    float skew_tol;          /* error-estimate tolerance of the fused pass */
+    uint64_t seed;
+} mpm_surrogate_train_options;
+
+void mpm_surrogate_default_train_options(mpm_surrogate_train_options *opt);
+
+/* Untrained network on a device (its envelope is empty: every particle
+ * falls back to the SVD until it is trained or loaded). */
+int mpm_surrogate_create(int device, uint64_t seed, mpm_surrogate **out);
+int mpm_surrogate_destroy(mpm_surrogate *s);
+
+/* Trains on the GPU from n_seed deformation gradients F_seed[n_seed*9]
+ * (row-major, e.g. the F plane of mpm_get_state after plain substeps).  opt
+ * may be NULL.  *final_loss (may be NULL) receives the last epoch's mean
+ * squared error in units of the output scale. */
+int mpm_surrogate_train(mpm_surrogate *s, const float *F_seed, int64_t n_seed,
+                        const mpm_surrogate_train_options *opt, float *final_loss);
+
+/* Kirchhoff stress divided by mu of n deformation gradients F[n*9] for
+ * lambda/mu = lam_over_mu: tau_pred from the network, tau_ref from the SVD
+ * path; accepted[i] = 1 where the fused pass would use the network.  Any
+ * output may be NULL. */
+int mpm_surrogate_eval(mpm_surrogate *s, const float *F, int64_t n, float lam_over_mu,
+                       float *tau_pred, float *tau_ref, uint8_t *accepted);
+
+/* Gradient of the mean squared error over 9 outputs of the batch
+ * (x[n*10] network inputs, y_target[n*9] targets, n a multiple of 128,
+ * n <= 2^20) with respect to the packed parameters, computed by the training
+ * kernels; grads[mpm_surrogate_num_params()], *loss may be NULL. */
+int mpm_surrogate_gradients(mpm_surrogate *s, const float *x, const float *y_target, int64_t n,
+                            float *grads, float *loss);
+
+/* Packed FP32 parameters: W1[64][16], W2[64][64], W3[16][64], b1[64],
+ * b2[64], b3[16] (padding rows and columns zero), and the model constants
+ * (in_scale, out_scale, env_c, env_jlo, env_jhi, skew_tol, tau_floor, pad). */
+int mpm_surrogate_num_params(void);
+int mpm_surrogate_num_meta(void);
+int mpm_surrogate_get_params(mpm_surrogate *s, float *params, float *meta);
+int mpm_surrogate_set_params(mpm_surrogate *s, const float *params, const float *meta);
+int mpm_surrogate_save(mpm_surrogate *s, const char *path);
+int mpm_surrogate_load(const char *path, int device, mpm_surrogate **out);
+
+/* Selects the stress of the 3D jello and snow groups: MPM_STRESS_PLAIN, or
+ * MPM_STRESS_SURROGATE with network s (kept alive by the caller while the
+ * handle uses it; call again after retraining s).  Needs MPM_P2G_ATOMIC;
+ * water and 2D scenes keep the plain stress. */
+int mpm_set_stress_mode(mpm_handle *h, int mode, mpm_surrogate *s);
+
+/* Particles whose stress came from the network / from the SVD fallback in
+ * surrogate mode since the mode was set. */
+int mpm_get_stress_stats(mpm_handle *h, int64_t *surrogate, int64_t *fallback);
 
 #ifdef __cplusplus
 }

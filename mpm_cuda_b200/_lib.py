@@ -51,6 +51,14 @@ class Options(C.Structure):
                 ("kernel_config", C.c_int)]
 
 
+class SurrogateTrainOptions(C.Structure):
+    _fields_ = [("n_samples", C.c_int64), ("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_float),
+                ("lr_final", C.c_float), ("sigma", C.c_float), ("rotation_fraction", C.c_float),
+                ("skew_tol", C.c_float), ("seed", C.c_uint64)]
+
+
+_U8P = C.POINTER(C.c_uint8)
+
 EXPORTS = {
     # name: (restype, argtypes)
     "mpm_default_options": (None, [C.POINTER(Options)]),
@@ -81,6 +89,21 @@ EXPORTS = {
     "mpm_set_kernel_config": (C.c_int, [C.c_void_p, C.c_int]),
     "mpm_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "mpm_step_noalloc": (C.c_int, [C.POINTER(SceneDesc), C.c_void_p, C.c_int64, C.c_int64, C.c_int, C.c_void_p]),
+    "mpm_surrogate_default_train_options": (None, [C.POINTER(SurrogateTrainOptions)]),
+    "mpm_surrogate_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "mpm_surrogate_destroy": (C.c_int, [C.c_void_p]),
+    "mpm_surrogate_train": (C.c_int, [C.c_void_p, _FP, C.c_int64, C.POINTER(SurrogateTrainOptions),
+                                      C.POINTER(C.c_float)]),
+    "mpm_surrogate_eval": (C.c_int, [C.c_void_p, _FP, C.c_int64, C.c_float, _FP, _FP, _U8P]),
+    "mpm_surrogate_gradients": (C.c_int, [C.c_void_p, _FP, _FP, C.c_int64, _FP, C.POINTER(C.c_float)]),
+    "mpm_surrogate_num_params": (C.c_int, []),
+    "mpm_surrogate_num_meta": (C.c_int, []),
+    "mpm_surrogate_get_params": (C.c_int, [C.c_void_p, _FP, _FP]),
+    "mpm_surrogate_set_params": (C.c_int, [C.c_void_p, _FP, _FP]),
+    "mpm_surrogate_save": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "mpm_surrogate_load": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "mpm_set_stress_mode": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "mpm_get_stress_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
 }
 
 _lib = None

@@ -17,6 +17,7 @@
 
 #include "mpm_config.cuh"
 #include "mpm_engine.cuh"
+#include "mpm_surrogate.cuh"
 
 namespace {
 
@@ -237,6 +238,16 @@ int mpm_set_p2g_mode(mpm_handle* h, int mode) {
     if (mode != MPM_P2G_ATOMIC && mode != MPM_P2G_DETERMINISTIC && mode != MPM_P2G_DIRECT)
         return fail(h, MPM_ERR_INVALID, "mpm_set_p2g_mode: bad mode %d", mode);
     return h->eng.set_p2g_mode(mode);
+}
+
+int mpm_set_stress_mode(mpm_handle* h, int mode, mpm_surrogate* s) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_set_stress_mode: NULL handle");
+    return h->eng.set_stress_mode(mode, mpm::surrogate_of(s));
+}
+
+int mpm_get_stress_stats(mpm_handle* h, int64_t* surrogate, int64_t* fallback) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_get_stress_stats: NULL handle");
+    return h->eng.stress_stats(surrogate, fallback);
 }
 
 int mpm_last_error(mpm_handle* h, char* buf, size_t cap) {

@@ -15,6 +15,8 @@
 #include "mpm_kernels_binned.cuh"
 #include "mpm_kernels_det.cuh"
 #include "mpm_kernels_direct.cuh"
+#include "mpm_kernels_surrogate.cuh"
+#include "mpm_surrogate.cuh"
 
 namespace mpm {
 
@@ -104,6 +106,18 @@ static void (*fused_fn(int dim, int mat, int ci))(ParticleBuf, FusedArgs) {
     return dim == 3 ? fused_for_mat<3>(mat, ci) : fused_for_mat<2>(mat, ci);
 }
 
+// the surrogate kernel closest to a fused-kernel configuration: 64 or 128
+// particles per CTA, at the lower or higher launch-bound occupancy
+template <int MAT>
+static void (*sur_for(const FusedCfg& c))(ParticleBuf, FusedArgs, SurArgs) {
+    if (c.chunk <= 64) return c.min_ctas >= 10 ? &k_g2p2g_sur<MAT, 64, 12> : &k_g2p2g_sur<MAT, 64, 8>;
+    return c.min_ctas >= 6 ? &k_g2p2g_sur<MAT, 128, 6> : &k_g2p2g_sur<MAT, 128, 4>;
+}
+static void (*sur_fn(int mat, int ci))(ParticleBuf, FusedArgs, SurArgs) {
+    return mat == SNOW ? sur_for<SNOW>(kFusedCfgs[ci]) : sur_for<JELLO>(kFusedCfgs[ci]);
+}
+static int sur_chunk(int ci) { return kFusedCfgs[ci].chunk <= 64 ? 64 : 128; }
+
 int Engine::cuda_fail(cudaError_t e, const char* what) {
     char buf[512];
     std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
@@ -138,7 +152,7 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
         return MPM_ERR_INVALID;
     }
     if (opt.stress_mode != MPM_STRESS_PLAIN) {
-        msg = "mpm_create: the surrogate stress needs a trained model (mpm_surrogate_load)";
+        msg = "mpm_create: select the surrogate stress with mpm_set_stress_mode after creation";
         return MPM_ERR_UNSUPPORTED;
     }
     char buf[512];
@@ -407,8 +421,22 @@ void Engine::set_config(int ci) {
         }
         fused_ctas[mat] = num_sms * std::max(1, per_sm);
     }
+    sur_occupancy();
     drop_graphs();
     grid_dirty = true;  // chunk lists depend on the chunk size
+}
+
+void Engine::sur_occupancy() {
+    for (int mat = 0; mat < kMats; ++mat) {
+        if (!sur_kernel(mat)) continue;
+        const int ch = sur_chunk(cfg);
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sur_fn(mat, cfg), ch, 0) != cudaSuccess) {
+            cudaGetLastError();
+            per_sm = 1;
+        }
+        sur_ctas[mat] = num_sms * std::max(1, per_sm);
+    }
 }
 
 namespace {
@@ -532,7 +560,7 @@ void Engine::release() {
     }
     void* ptrs[] = {groups_d, scenes_d, grid_mom, grid_vel, err_d, keys[0], keys[1], vals[0], vals[1],
                     cell_count, seg_count, seg_start, sort_tmp, blk_flag, active, blk_epoch, counters, chunks,
-                    scan_tmp, pos_out, cell_end, det_src};
+                    scan_tmp, pos_out, cell_end, det_src, sur_counts};
     for (void* p : ptrs) cudaFree(p);
     groups_d = nullptr;
     scenes_d = nullptr;
@@ -548,6 +576,8 @@ void Engine::release() {
     chunks = nullptr;
     scan_tmp = nullptr;
     pos_out = nullptr;
+    sur_counts = nullptr;
+    sur = nullptr;
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
 }
@@ -668,8 +698,15 @@ void Engine::enqueue_g2p2g(int parity) {
         if (!mat_present[mat]) continue;
         const FusedArgs A = fused_args(mat, bump);
         bump = false;
-        fused_fn(dim, mat, cfg)<<<fused_ctas[mat], kFusedCfgs[cfg].chunk, 0, stream>>>(buf(parity), A);
-        note_launch("fused_fn");
+        if (sur_kernel(mat)) {
+            const SurArgs SA{&sur->weights->f, sur->meta, sur_counts};
+            const int ch = sur_chunk(cfg);
+            sur_fn(mat, cfg)<<<sur_ctas[mat], ch, 0, stream>>>(buf(parity), A, SA);
+            note_launch("k_g2p2g_sur");
+        } else {
+            fused_fn(dim, mat, cfg)<<<fused_ctas[mat], kFusedCfgs[cfg].chunk, 0, stream>>>(buf(parity), A);
+            note_launch("fused_fn");
+        }
     }
 }
 
@@ -814,6 +851,7 @@ int Engine::step(int n) {
         return MPM_ERR_INVALID;
     }
     MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    sur_refresh();
     if (direct()) {
         if (grid_dirty) {
             MPM_CUDA_TRY(cudaMemsetAsync(grid_mom, 0, (size_t)total_blocks * 64 * sizeof(float4), stream),
@@ -1066,10 +1104,69 @@ int Engine::bin_stats(int64_t* fallbacks, int64_t* rebins) {
 }
 
 int Engine::set_p2g_mode(int mode) {
+    if (sur && mode != MPM_P2G_ATOMIC) {
+        last_error = "mpm_set_p2g_mode: the surrogate stress runs in MPM_P2G_ATOMIC only";
+        return MPM_ERR_UNSUPPORTED;
+    }
     MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
     opt.p2g_mode = mode;
     drop_graphs();
     grid_dirty = true;
+    return MPM_OK;
+}
+
+int Engine::set_stress_mode(int mode, Surrogate* s) {
+    if (mode != MPM_STRESS_PLAIN && mode != MPM_STRESS_SURROGATE) {
+        last_error = "mpm_set_stress_mode: bad mode";
+        return MPM_ERR_INVALID;
+    }
+    if (mode == MPM_STRESS_SURROGATE) {
+        if (!s) {
+            last_error = "mpm_set_stress_mode: MPM_STRESS_SURROGATE needs a surrogate";
+            return MPM_ERR_INVALID;
+        }
+        if (!fused()) {
+            last_error = "mpm_set_stress_mode: the surrogate stress runs in MPM_P2G_ATOMIC only";
+            return MPM_ERR_UNSUPPORTED;
+        }
+        if (s->device != device) {
+            last_error = "mpm_set_stress_mode: surrogate and handle are on different devices";
+            return MPM_ERR_INVALID;
+        }
+    }
+    MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
+    if (!sur_counts) MPM_CUDA_TRY(cudaMalloc((void**)&sur_counts, 2 * sizeof(unsigned long long)), "alloc counters");
+    MPM_CUDA_TRY(cudaMemset(sur_counts, 0, 2 * sizeof(unsigned long long)), "clear counters");
+    sur = mode == MPM_STRESS_SURROGATE ? s : nullptr;
+    opt.stress_mode = mode;
+    // eligible groups: 3D jello and snow
+    for (auto& g : groups_h) g.surrogate = (sur && dim == 3 && (g.type == JELLO || g.type == SNOW)) ? 1 : 0;
+    MPM_CUDA_TRY(cudaMemcpy(groups_d, groups_h.data(), groups_h.size() * sizeof(GroupParams), cudaMemcpyHostToDevice),
+                 "group upload");
+    sur_version = sur ? sur->version : -1;
+    sur_occupancy();
+    drop_graphs();
+    return MPM_OK;
+}
+
+// captured graphs hold the network's constants by value: re-capture after a
+// retraining or set_params
+int Engine::sur_refresh() {
+    if (sur && sur->version != sur_version) {
+        sur_version = sur->version;
+        drop_graphs();
+    }
+    return MPM_OK;
+}
+
+int Engine::stress_stats(int64_t* net, int64_t* fallback) {
+    MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
+    unsigned long long c[2] = {0ull, 0ull};
+    if (sur_counts) MPM_CUDA_TRY(cudaMemcpy(c, sur_counts, sizeof(c), cudaMemcpyDeviceToHost), "counter download");
+    if (net) *net = (int64_t)c[0];
+    if (fallback) *fallback = (int64_t)c[1];
     return MPM_OK;
 }
 
@@ -1086,16 +1183,22 @@ int Engine::profile_stages(int n, float* out_ms, int n_out, int* n_written) {
             int rc = prologue();
             if (rc != MPM_OK) return rc;
         }
-        // one re-binning
-        cudaEventRecord(ev[0], stream);
-        enqueue_rebin(cur);
-        cudaEventRecord(ev[1], stream);
-        cudaEventSynchronize(ev[1]);
-        cudaEventElapsedTime(&acc[0], ev[0], ev[1]);
-        cur = 1 - cur;
-        steps_since_rebin = 0;
-        acc[0] *= n;
+        // re-binnings at the handle's interval, as in step(); reported per
+        // re-binning, the other stages per substep
+        int n_rebin = 0;
         for (int it = 0; it < n; ++it) {
+            if (it == 0 || steps_since_rebin >= opt.rebin_interval) {
+                cudaEventRecord(ev[0], stream);
+                enqueue_rebin(cur);
+                cudaEventRecord(ev[1], stream);
+                cudaEventSynchronize(ev[1]);
+                float r = 0.f;
+                cudaEventElapsedTime(&r, ev[0], ev[1]);
+                acc[0] += r;
+                ++n_rebin;
+                cur = 1 - cur;
+                steps_since_rebin = 0;
+            }
             cudaEventRecord(ev[0], stream);
             enqueue_grid_update();
             cudaEventRecord(ev[1], stream);
@@ -1109,6 +1212,7 @@ int Engine::profile_stages(int n, float* out_ms, int n_out, int* n_written) {
             acc[2] += b;
             ++steps_since_rebin;
         }
+        acc[0] *= (float)n / (float)n_rebin;
     } else if (deterministic()) {
         if (grid_dirty) {
             int rc = prologue();

@@ -15,6 +15,7 @@ int write_bgeo(const char* path, const float* x, int64_t n, int dim);
 
 struct Chunk;
 struct FusedArgs;
+struct Surrogate;
 
 struct Engine {
     int dim = 3;
@@ -69,6 +70,13 @@ struct Engine {
     float* pos_out = nullptr;  // gathered positions (creation order)
     int fused_ctas[3] = {0, 0, 0};  // persistent CTAs per material kernel
     int cfg = 1;                     // index into kFusedCfgs
+    // learned stress (MPM_STRESS_SURROGATE): the network, the version of its
+    // weights the graphs were captured with, per-material persistent CTAs and
+    // the network / fallback counters
+    Surrogate* sur = nullptr;
+    long long sur_version = -1;
+    int sur_ctas[3] = {0, 0, 0};
+    unsigned long long* sur_counts = nullptr;
     int update_ctas = 0;
     int steps_since_rebin = 0;
 
@@ -93,6 +101,8 @@ struct Engine {
     int get_grid(int scene, float* mass, float* vel);
     int count_active_nodes(int scene, int64_t* n);
     int set_p2g_mode(int mode);
+    int set_stress_mode(int mode, Surrogate* s);
+    int stress_stats(int64_t* net, int64_t* fallback);
     int profile_stages(int n, float* out_ms, int n_out, int* n_written);
     int get_positions(int scene, float* out);
     int bin_stats(int64_t* fallbacks, int64_t* rebins);
@@ -118,6 +128,9 @@ struct Engine {
     bool fused() const { return opt.p2g_mode == MPM_P2G_ATOMIC; }
     bool deterministic() const { return opt.p2g_mode == MPM_P2G_DETERMINISTIC; }
     bool direct() const { return opt.p2g_mode == MPM_P2G_DIRECT; }
+    bool sur_kernel(int mat) const { return sur && dim == 3 && (mat == JELLO || mat == SNOW); }
+    void sur_occupancy();
+    int sur_refresh();
     void enqueue_det_p2g();
     void enqueue_det_substep();
     int canonical_order();

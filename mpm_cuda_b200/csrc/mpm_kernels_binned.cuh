@@ -267,6 +267,150 @@ __device__ __forceinline__ int tm_idx(int x, int y, int z) {
     return x + TileShape<D>::MY * y + TileShape<D>::MZ * z;
 }
 
+// ---- pieces of the fused pass (shared by the plain and surrogate kernels)
+
+// window origin of a chunk's home block: one node below the block
+template <int D>
+__device__ __forceinline__ void tile_origin(const SceneParams& sc, long long lb, int* o) {
+    constexpr int SIDE = TileShape<D>::SIDE;
+    o[0] = (int)(lb % sc.nb[0]) * SIDE - 1;
+    o[1] = (int)((lb / sc.nb[0]) % sc.nb[1]) * SIDE - 1;
+    o[2] = (D == 3) ? (int)(lb / ((long long)sc.nb[0] * sc.nb[1])) * SIDE - 1 : 0;
+}
+
+// grid velocity window of a chunk (zero outside the grid), NT threads
+template <int D, int NT>
+__device__ __forceinline__ void load_velocity_tile(const SceneParams& sc, const int* o, const float4* __restrict__ grid_vel,
+                                                   float4* tv) {
+    constexpr int T = TileShape<D>::T;
+    for (int t = threadIdx.x; t < TileShape<D>::N; t += NT) {
+        const int tx = t % T, ty = (t / T) % T, tz = (D == 3) ? t / (T * T) : 0;
+        const int ix = o[0] + tx, iy = o[1] + ty, iz = o[2] + tz;
+        bool in = ix >= 0 && iy >= 0 && ix < sc.n[0] && iy < sc.n[1];
+        if (D == 3) in = in && iz >= 0 && iz < sc.n[2];
+        tv[tv_idx<D>(tx, ty, tz)] = in ? grid_vel[node_index<D>(sc, ix, iy, iz)] : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
+// true when the stencil at `base` lies inside the chunk's window
+template <int D>
+__device__ __forceinline__ bool in_window(const int* base, const int* o) {
+    bool in = true;
+#pragma unroll
+    for (int a = 0; a < D; ++a) in = in && (base[a] - o[a] >= 0) && (base[a] - o[a] <= TileShape<D>::T - 3);
+    return in;
+}
+
+// G2P of one particle from the window, or from global memory for a particle
+// that drifted out of it since the last re-binning
+template <int D>
+__device__ __forceinline__ void g2p_window(const Stencil<D>& st, const int* o, const float4* tv, const SceneParams& sc,
+                                           const FusedArgs& A, G2PAcc<D>& acc) {
+    if (in_window<D>(st.base, o)) {
+        const int b0 = st.base[0] - o[0], b1 = st.base[1] - o[1], b2 = D == 3 ? st.base[2] - o[2] : 0;
+        g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) {
+            return tv[tv_idx<D>(b0 + ox, b1 + oy, b2 + oz)];
+        }, acc);
+    } else {
+        atomicAdd(A.fallback, 1u);
+        g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) {
+            return A.grid_vel[node_index<D>(sc, st.base[0] + ox, st.base[1] + oy, D == 3 ? st.base[2] + oz : 0)];
+        }, acc);
+    }
+}
+
+// Particle update after G2P (F / Jp / J, advection, new C) and store of the
+// new state; x, v, Cn, F, aux hold it on return.
+template <int D, int MAT>
+__device__ __forceinline__ unsigned update_and_store(const G2PAcc<D>& acc, const SceneParams& sc, const GroupParams& g,
+                                                     float* __restrict__ S, long long cap, long long i, float* x,
+                                                     float* v, float* Cn, float* F, float& aux) {
+    using P = Planes<D>;
+    aux = 1.f;
+    if (MAT != JELLO) aux = S[P::AUX * cap + i];
+    if (MAT != WATER) {
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) F[k] = S[(P::F + k) * cap + i];
+    } else {
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) F[k] = (k % (D + 1) == 0) ? 1.f : 0.f;
+    }
+    const unsigned err = material_update<D, MAT>(acc, sc.dt, g, F, aux);
+    const float c4 = 4.f * sc.inv_h;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        v[a] = acc.v[a];
+        x[a] = fmaf(sc.dt, acc.v[a], x[a]);
+#pragma unroll
+        for (int b = 0; b < D; ++b) Cn[a * D + b] = c4 * acc.B[a * D + b];
+    }
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        S[(P::X + a) * cap + i] = x[a];
+        S[(P::V + a) * cap + i] = v[a];
+    }
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) S[(P::C + k) * cap + i] = Cn[k];
+    if (MAT != WATER) {
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) S[(P::F + k) * cap + i] = F[k];
+    }
+    if (MAT != JELLO) S[P::AUX * cap + i] = aux;
+    return err;
+}
+
+// neighbour-block slots covered by a stencil whose base is local node l of
+// the window: the window starts one node below the home block, so local node
+// l lies in block slot (l + SIDE - 1) / SIDE (0: home - 1, 1: home, 2: home + 1)
+template <int D>
+__device__ __forceinline__ unsigned touched_bits(int l0, int l1, int l2) {
+    constexpr int SIDE = TileShape<D>::SIDE;
+    unsigned bits = 0u;
+#pragma unroll
+    for (int cx = 0; cx < 2; ++cx)
+#pragma unroll
+        for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+            for (int cz = 0; cz < (D == 3 ? 2 : 1); ++cz) {
+                const int sx = (l0 + 2 * cx + SIDE - 1) / SIDE;
+                const int sy = (l1 + 2 * cy + SIDE - 1) / SIDE;
+                const int sz = D == 3 ? (l2 + 2 * cz + SIDE - 1) / SIDE : 0;
+                bits |= 1u << (sx + 3 * (sy + 3 * sz));
+            }
+    return bits;
+}
+
+// P2G scatter of the next substep straight to global memory with float4
+// reductions; a stencil inside the window records the blocks it covers in
+// `touched`, one outside it marks them itself
+template <int D>
+__device__ __forceinline__ void scatter_global(const Stencil<D>& sn, const P2GSource<D>& src, const SceneParams& sc,
+                                               const int* o, const FusedArgs& A, unsigned* touched) {
+    if (in_window<D>(sn.base, o)) {
+        p2g_scatter<D>(sn, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 cc) {
+            atomicAdd(&A.grid_mom[node_index<D>(sc, sn.base[0] + ox, sn.base[1] + oy, D == 3 ? sn.base[2] + oz : 0)],
+                      cc);
+        });
+        atomicOr(touched, touched_bits<D>(sn.base[0] - o[0], sn.base[1] - o[1], D == 3 ? sn.base[2] - o[2] : 0));
+    } else {
+        atomicAdd(A.fallback, 1u);
+        p2g_global<D>(sn, src, sc, A.grid_mom, A.blk_flag, A.active, A.n_active);
+    }
+}
+
+// marks the neighbour blocks recorded in `touched` (threads 0 .. 3^D - 1)
+template <int D>
+__device__ __forceinline__ void mark_touched(unsigned touched, const SceneParams& sc, const int* o, const FusedArgs& A) {
+    constexpr int SIDE = TileShape<D>::SIDE;
+    if ((int)threadIdx.x < (D == 3 ? 27 : 9) && ((touched >> threadIdx.x) & 1u)) {
+        const int sx = threadIdx.x % 3, sy = (threadIdx.x / 3) % 3, sz = threadIdx.x / 9;
+        const long long bx = (o[0] + 1) / SIDE - 1 + sx, by = (o[1] + 1) / SIDE - 1 + sy;
+        const long long bz = D == 3 ? (o[2] + 1) / SIDE - 1 + sz : 0;
+        const long long gb = sc.block_off + bx + (long long)sc.nb[0] * (by + (long long)sc.nb[1] * bz);
+        mark_block(A.blk_flag, A.active, A.n_active, gb);
+    }
+}
+
 // One substep for the particles of each chunk of material MAT: G2P from the
 // velocity tile, F / Jp / J update, advection, stress, and P2G of the next
 // substep (MPMCUDA.cu:310-741 in one pass: the reference runs P2G, VelUpdate
@@ -283,7 +427,6 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
     using TS = TileShape<D>;
     constexpr int T = TS::T;
     constexpr int TN = TS::N;
-    constexpr int SIDE = TS::SIDE;
     constexpr int MN = SCAT == 0 ? TS::MN : 1;
     __shared__ float4 tv[TS::VN];  // grid velocity window
     __shared__ float tm[4][MN];    // next-substep momentum / mass window (SCAT 0)
@@ -301,20 +444,13 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
         const Chunk ch = A.chunks[c];
         const int s = scene_of_block(A.scenes, A.n_scenes, ch.block);
         const SceneParams& sc = A.scenes[s];
-        const long long lb = ch.block - sc.block_off;
         int o[3];
-        o[0] = (int)(lb % sc.nb[0]) * SIDE - 1;
-        o[1] = (int)((lb / sc.nb[0]) % sc.nb[1]) * SIDE - 1;
-        o[2] = (D == 3) ? (int)(lb / ((long long)sc.nb[0] * sc.nb[1])) * SIDE - 1 : 0;
+        tile_origin<D>(sc, ch.block - sc.block_off, o);
         if (threadIdx.x == 0) touched = 0u;
-        for (int t = threadIdx.x; t < TN; t += CHUNK) {
-            const int tx = t % T, ty = (t / T) % T, tz = (D == 3) ? t / (T * T) : 0;
-            const int ix = o[0] + tx, iy = o[1] + ty, iz = o[2] + tz;
-            bool in = ix >= 0 && iy >= 0 && ix < sc.n[0] && iy < sc.n[1];
-            if (D == 3) in = in && iz >= 0 && iz < sc.n[2];
-            tv[tv_idx<D>(tx, ty, tz)] = in ? A.grid_vel[node_index<D>(sc, ix, iy, iz)] : make_float4(0.f, 0.f, 0.f, 0.f);
-            if (SCAT == 0) {
-                const int m = tm_idx<D>(tx, ty, tz);
+        load_velocity_tile<D, CHUNK>(sc, o, A.grid_vel, tv);
+        if (SCAT == 0) {
+            for (int t = threadIdx.x; t < TN; t += CHUNK) {
+                const int m = tm_idx<D>(t % T, (t / T) % T, (D == 3) ? t / (T * T) : 0);
                 tm[0][m] = 0.f;
                 tm[1][m] = 0.f;
                 tm[2][m] = 0.f;
@@ -334,68 +470,20 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
             for (int a = 0; a < D; ++a) x[a] = S[(P::X + a) * cap + i];
             Stencil<D> st;
             if (make_stencil<D>(x, sc, st, err)) {
-                // ---- G2P
                 G2PAcc<D> acc;
-                bool local = true;
-#pragma unroll
-                for (int a = 0; a < D; ++a) local = local && (st.base[a] - o[a] >= 0) && (st.base[a] - o[a] <= T - 3);
-                if (local) {
-                    const int b0 = st.base[0] - o[0], b1 = st.base[1] - o[1], b2 = D == 3 ? st.base[2] - o[2] : 0;
-                    g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) {
-                        return tv[tv_idx<D>(b0 + ox, b1 + oy, b2 + oz)];
-                    }, acc);
-                } else {
-                    atomicAdd(A.fallback, 1u);
-                    g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) {
-                        return A.grid_vel[node_index<D>(sc, st.base[0] + ox, st.base[1] + oy,
-                                                        D == 3 ? st.base[2] + oz : 0)];
-                    }, acc);
-                }
-                // ---- particle update
-                float F[D * D], Cn[D * D], v[D];
-                float aux = 1.f;
-                if (MAT != JELLO) aux = S[P::AUX * cap + i];
-                if (MAT != WATER) {
-#pragma unroll
-                    for (int k = 0; k < D * D; ++k) F[k] = S[(P::F + k) * cap + i];
-                } else {
-#pragma unroll
-                    for (int k = 0; k < D * D; ++k) F[k] = (k % (D + 1) == 0) ? 1.f : 0.f;
-                }
-                err |= material_update<D, MAT>(acc, sc.dt, g, F, aux);
-                const float c4 = 4.f * sc.inv_h;
-#pragma unroll
-                for (int a = 0; a < D; ++a) {
-                    v[a] = acc.v[a];
-                    x[a] = fmaf(sc.dt, acc.v[a], x[a]);
-#pragma unroll
-                    for (int b = 0; b < D; ++b) Cn[a * D + b] = c4 * acc.B[a * D + b];
-                }
-#pragma unroll
-                for (int a = 0; a < D; ++a) {
-                    S[(P::X + a) * cap + i] = x[a];
-                    S[(P::V + a) * cap + i] = v[a];
-                }
-#pragma unroll
-                for (int k = 0; k < D * D; ++k) S[(P::C + k) * cap + i] = Cn[k];
-                if (MAT != WATER) {
-#pragma unroll
-                    for (int k = 0; k < D * D; ++k) S[(P::F + k) * cap + i] = F[k];
-                }
-                if (MAT != JELLO) S[P::AUX * cap + i] = aux;
+                g2p_window<D>(st, o, tv, sc, A, acc);
+                float F[D * D], Cn[D * D], v[D], aux;
+                err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux);
 
                 // ---- stress + P2G of the next substep
                 Stencil<D> sn;
                 if (make_stencil<D>(x, sc, sn, err)) {
                     P2GSource<D> src;
                     particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc, src);
-                    bool in_tile = true;
-#pragma unroll
-                    for (int a = 0; a < D; ++a)
-                        in_tile = in_tile && (sn.base[a] - o[a] >= 0) && (sn.base[a] - o[a] <= T - 3);
-                    if (in_tile) {
-                        const int l0 = sn.base[0] - o[0], l1 = sn.base[1] - o[1], l2 = D == 3 ? sn.base[2] - o[2] : 0;
-                        if (SCAT == 0) {
+                    if (SCAT == 0) {
+                        if (in_window<D>(sn.base, o)) {
+                            const int l0 = sn.base[0] - o[0], l1 = sn.base[1] - o[1],
+                                      l2 = D == 3 ? sn.base[2] - o[2] : 0;
                             p2g_scatter<D>(sn, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 cc) {
                                 const int m = tm_idx<D>(l0 + ox, l1 + oy, l2 + oz);
                                 atomicAdd(&tm[0][m], cc.x);
@@ -403,32 +491,13 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
                                 if (D == 3) atomicAdd(&tm[2][m], cc.z);
                                 atomicAdd(&tm[3][m], cc.w);
                             });
+                            atomicOr(&touched, touched_bits<D>(l0, l1, l2));
                         } else {
-                            p2g_scatter<D>(sn, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 cc) {
-                                atomicAdd(&A.grid_mom[node_index<D>(sc, sn.base[0] + ox, sn.base[1] + oy,
-                                                                    D == 3 ? sn.base[2] + oz : 0)],
-                                          cc);
-                            });
+                            atomicAdd(A.fallback, 1u);
+                            p2g_global<D>(sn, src, sc, A.grid_mom, A.blk_flag, A.active, A.n_active);
                         }
-                        // neighbour-block slots covered by the stencil: the window starts
-                        // one node below the home block, so local node l lies in block slot
-                        // (l + SIDE - 1) / SIDE (0: home - 1, 1: home, 2: home + 1)
-                        unsigned bits = 0u;
-#pragma unroll
-                        for (int cx = 0; cx < 2; ++cx)
-#pragma unroll
-                            for (int cy = 0; cy < 2; ++cy)
-#pragma unroll
-                                for (int cz = 0; cz < (D == 3 ? 2 : 1); ++cz) {
-                                    const int sx = (l0 + 2 * cx + SIDE - 1) / SIDE;
-                                    const int sy = (l1 + 2 * cy + SIDE - 1) / SIDE;
-                                    const int sz = D == 3 ? (l2 + 2 * cz + SIDE - 1) / SIDE : 0;
-                                    bits |= 1u << (sx + 3 * (sy + 3 * sz));
-                                }
-                        atomicOr(&touched, bits);
                     } else {
-                        atomicAdd(A.fallback, 1u);
-                        p2g_global<D>(sn, src, sc, A.grid_mom, A.blk_flag, A.active, A.n_active);
+                        scatter_global<D>(sn, src, sc, o, A, &touched);
                     }
                 }
             }
@@ -448,13 +517,7 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
                               make_float4(mx, my, mz, mm));
             }
         }
-        if ((int)threadIdx.x < (D == 3 ? 27 : 9) && ((touched >> threadIdx.x) & 1u)) {
-            const int sx = threadIdx.x % 3, sy = (threadIdx.x / 3) % 3, sz = threadIdx.x / 9;
-            const long long bx = (o[0] + 1) / SIDE - 1 + sx, by = (o[1] + 1) / SIDE - 1 + sy;
-            const long long bz = D == 3 ? (o[2] + 1) / SIDE - 1 + sz : 0;
-            const long long gb = sc.block_off + bx + (long long)sc.nb[0] * (by + (long long)sc.nb[1] * bz);
-            mark_block(A.blk_flag, A.active, A.n_active, gb);
-        }
+        mark_touched<D>(touched, sc, o, A);
         __syncthreads();
     }
 }

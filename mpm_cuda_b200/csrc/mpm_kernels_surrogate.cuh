@@ -1,0 +1,153 @@
+// Fused substep with the learned stress (MPM_STRESS_SURROGATE), 3D jello and
+// snow.  Same pass as k_g2p2g (G2P, particle update, stress, P2G of the next
+// substep) with the stress of eligible particles taken from the BF16 MLP
+// (mpm_mlp.cuh) instead of the SVD in kirchhoff_fcr (MPMCUDA.cu:229-264):
+//   1. every thread: G2P, update, store the new state, write its network
+//      input (X = F F^T - I, J - 1) to a shared row;
+//   2. every warp: forward pass of its 32 rows on the tensor cores, in place;
+//   3. every thread: re-read its new state (from L2), stress from the
+//      prediction when F is inside the training envelope and the error
+//      estimate is below tolerance, else from the SVD; scatter.
+// The state is re-read instead of kept live so that the network's registers
+// do not add to the G2P registers.
+#pragma once
+
+#include "mpm_kernels_binned.cuh"
+#include "mpm_mlp.cuh"
+
+namespace mpm {
+
+struct SurArgs {
+    const mlp::Forward* weights;
+    mlp::Meta meta;
+    unsigned long long* counts;  // [0] stresses from the network, [1] SVD fallbacks
+};
+
+template <int MAT, int CHUNK, int MINB>
+__global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, FusedArgs A, SurArgs SA) {
+    constexpr int D = 3;
+    using P = Planes<D>;
+    using TS = TileShape<D>;
+    static_assert(CHUNK % 32 == 0, "whole warps");
+    static_assert(MAT == JELLO || MAT == SNOW, "elastic materials only");
+    __shared__ float4 tv[TS::VN];                      // grid velocity window
+    __shared__ __align__(16) mlp::Forward W;           // network weights
+    constexpr int XS = mlp::IN_PAD + 1;  // odd row stride: per-particle rows hit 32 banks
+    __shared__ float sxy[CHUNK * XS];     // network inputs, then outputs
+    __shared__ unsigned touched;
+    __shared__ int s_chunk;
+
+    if (A.bump_epoch && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.epoch, 1);
+    {
+        const int4* src = reinterpret_cast<const int4*>(SA.weights);
+        int4* dst = reinterpret_cast<int4*>(&W);
+        for (int k = threadIdx.x; k < (int)(sizeof(mlp::Forward) / 16); k += CHUNK) dst[k] = src[k];
+    }
+    const int lane = threadIdx.x & 31, w0 = threadIdx.x & ~31;
+    unsigned n_net = 0, n_svd = 0;
+    const int nch = *A.n_chunks;
+    for (;;) {
+        if (threadIdx.x == 0) s_chunk = atomicAdd(A.cursor, 1);
+        __syncthreads();  // also publishes W on the first pass
+        const int c = s_chunk;
+        if (c >= nch) break;
+        const Chunk ch = A.chunks[c];
+        const int s = scene_of_block(A.scenes, A.n_scenes, ch.block);
+        const SceneParams& sc = A.scenes[s];
+        int o[3];
+        tile_origin<D>(sc, ch.block - sc.block_off, o);
+        if (threadIdx.x == 0) touched = 0u;
+        load_velocity_tile<D, CHUNK>(sc, o, A.grid_vel, tv);
+        __syncthreads();
+
+        const long long i = (long long)ch.start + threadIdx.x;
+        float* S = pb.s;
+        const long long cap = pb.cap;
+        unsigned err = 0;
+        bool next = false;      // the particle scatters into the next substep
+        bool eligible = false;  // its group takes the network's stress
+        int gi = 0;             // its group (re-read after the network: fewer live registers)
+        float* row = sxy + threadIdx.x * XS;
+        if ((int)threadIdx.x < ch.count) {
+            gi = pb.grp[i];
+            const GroupParams g = A.groups[gi];
+            float x[D];
+#pragma unroll
+            for (int a = 0; a < D; ++a) x[a] = S[(P::X + a) * cap + i];
+            Stencil<D> st;
+            if (make_stencil<D>(x, sc, st, err)) {
+                G2PAcc<D> acc;
+                g2p_window<D>(st, o, tv, sc, A, acc);
+                float F[D * D], Cn[D * D], v[D], aux;
+                err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux);
+                Stencil<D> sn;
+                next = make_stencil<D>(x, sc, sn, err);
+                eligible = next && g.surrogate != 0;
+                if (eligible) mlp::features(F, det<3>(F), SA.meta, row);
+            }
+        }
+        if (!eligible) {
+#pragma unroll
+            for (int k = 0; k < mlp::IN_PAD; ++k) row[k] = 0.f;
+        }
+        __syncwarp();
+        // ---- network: 32 rows per warp, two 16-row tiles, in place
+        if (__any_sync(0xffffffffu, eligible)) {
+            mlp::forward_tile<XS>(W, sxy + w0 * XS, sxy + w0 * XS, lane);
+            mlp::forward_tile<XS>(W, sxy + (w0 + 16) * XS, sxy + (w0 + 16) * XS, lane);
+        }
+        __syncwarp();
+        if (next) {
+            // the state stored above, read back through L2
+            float x[D], v[D], Cn[D * D], F[D * D], aux = 1.f;
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                x[a] = __ldcg(S + (P::X + a) * cap + i);
+                v[a] = __ldcg(S + (P::V + a) * cap + i);
+            }
+#pragma unroll
+            for (int k = 0; k < D * D; ++k) {
+                Cn[k] = __ldcg(S + (P::C + k) * cap + i);
+                F[k] = __ldcg(S + (P::F + k) * cap + i);
+            }
+            if (MAT == SNOW) aux = __ldcg(S + P::AUX * cap + i);
+            const GroupParams g = A.groups[gi];
+            Stencil<D> sn;
+            make_stencil<D>(x, sc, sn, err);  // the stencil found in phase 1
+            float tau[D * D];
+            bool use = false;
+            if (eligible) {
+                float mu = g.mu, la = g.lambda;
+                if (MAT == SNOW) {
+                    // hardening exp(xi (1 - Jp)) (MPMCUDA.cu:342-347)
+                    const float hc = expf(g.xi * (1.f - aux));
+                    mu *= hc;
+                    la *= hc;
+                }
+                const float J = det<3>(F);
+                use = mlp::in_envelope(F, J, SA.meta) && mlp::tau_from_prediction(row, F, J, mu, la, SA.meta, tau);
+            }
+            P2GSource<D> src;
+            if (use) {
+                source_from_tau<D>(v, Cn, tau, g, sc, src);
+                ++n_net;
+            } else {
+                particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc, src);
+                ++n_svd;
+            }
+            scatter_global<D>(sn, src, sc, o, A, &touched);
+        }
+        if (err) atomicOr(A.err_word, err);
+        __syncthreads();
+        mark_touched<D>(touched, sc, o, A);
+        __syncthreads();
+    }
+    n_net = __reduce_add_sync(0xffffffffu, n_net);
+    n_svd = __reduce_add_sync(0xffffffffu, n_svd);
+    if (lane == 0 && (n_net | n_svd)) {
+        atomicAdd(&SA.counts[0], (unsigned long long)n_net);
+        atomicAdd(&SA.counts[1], (unsigned long long)n_svd);
+    }
+}
+
+}  // namespace mpm

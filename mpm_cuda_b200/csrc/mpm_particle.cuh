@@ -99,6 +99,21 @@ __device__ __forceinline__ void particle_stress_source(const float* v, const flo
     src.m = g.p_mass;
 }
 
+// the same source from a given Kirchhoff stress (the surrogate path)
+template <int D>
+__device__ __forceinline__ void source_from_tau(const float* v, const float* C, const float* tau, const GroupParams& g,
+                                                const SceneParams& sc, P2GSource<D>& src) {
+    const float k = -sc.dt * g.p_vol;
+#pragma unroll
+    for (int i = 0; i < D * D; ++i) {
+        src.A[i] = k * tau[i];
+        src.mC[i] = g.p_mass * C[i];
+    }
+#pragma unroll
+    for (int a = 0; a < D; ++a) src.mv[a] = g.p_mass * v[a];
+    src.m = g.p_mass;
+}
+
 // contribution of the source to stencil node `o` (offsets 0..2 per axis)
 template <int D>
 __device__ __forceinline__ float4 p2g_node(const Stencil<D>& st, const P2GSource<D>& src,

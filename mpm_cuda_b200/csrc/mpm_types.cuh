@@ -20,7 +20,7 @@ struct GroupParams {
     float xi, theta_c, theta_s;
     float bulk_k, gamma;
     float p_mass, p_vol;
-    int pad;
+    int surrogate;  // stress from the learned surrogate (MPM_STRESS_SURROGATE)
 };
 
 // One scene's grid and integration constants (Grid, MPMSimulator.cuh:54-64).

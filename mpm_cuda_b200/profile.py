@@ -35,17 +35,27 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--rebin-interval", type=int, default=0)
     ap.add_argument("--kernel-config", type=int, default=-1, help="-1 = autotune")
+    ap.add_argument("--surrogate", default=None, help="trained surrogate file: run with the network stress")
     args = ap.parse_args()
     scenes = WORKLOADS[args.workload]()
+    sur = None
     with Simulation(scenes, p2g_mode=MODES[args.mode], rebin_interval=args.rebin_interval,
                     kernel_config=args.kernel_config) as sim:
+        if args.surrogate:
+            from .surrogate import StressSurrogate
+            sur = StressSurrogate.load(args.surrogate)
+            sim.set_stress_mode(L.STRESS_SURROGATE, sur)
         sim.step(args.warmup)
         sim.step(args.steps)
         stages = sim.profile_stages(max(1, args.steps))
         fb, rb = sim.bin_stats()
         print(json.dumps({"workload": args.workload, "mode": args.mode, "kernel_config": sim.kernel_config(),
                           "particles": sim.num_particles(),
-                          "stage_ms": [round(s, 5) for s in stages], "tile_fallbacks": fb, "rebins": rb}))
+                          "stage_ms": [round(s, 5) for s in stages], "tile_fallbacks": fb, "rebins": rb,
+                          "stress": "surrogate" if sur else "plain",
+                          "network_fallback": list(sim.stress_stats()) if sur else None}))
+    if sur:
+        sur.close()
 
 
 if __name__ == "__main__":

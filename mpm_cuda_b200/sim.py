@@ -203,6 +203,18 @@ class Simulation:
     def set_p2g_mode(self, mode: int):
         self._check(self._lib.mpm_set_p2g_mode(self._h, mode))
 
+    def set_stress_mode(self, mode: int, surrogate=None):
+        """MPM_STRESS_PLAIN, or MPM_STRESS_SURROGATE with a trained
+        ``StressSurrogate`` (kept alive by this object while it is in use)."""
+        self._surrogate = surrogate if mode == L.STRESS_SURROGATE else None
+        self._check(self._lib.mpm_set_stress_mode(self._h, mode, surrogate.handle if surrogate else None))
+
+    def stress_stats(self):
+        """(stresses from the network, SVD fallbacks) since the mode was set."""
+        a, b = C.c_int64(), C.c_int64()
+        self._check(self._lib.mpm_get_stress_stats(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def time(self):
         t, f = C.c_double(), C.c_int64()
         self._check(self._lib.mpm_get_time(self._h, C.byref(t), C.byref(f)))
