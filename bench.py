@@ -42,6 +42,9 @@ METRIC = "particle-substeps/sec @1 B200, surrogate vs plain at stated stress/pos
 UNIT = "particle-substeps/s"
 L2_FLUSH_BYTES = 256 << 20
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# plain-run substeps at which the surrogate's training set is harvested:
+# start, interval, snapshots, held-out offset after the last
+SURROGATE_HARVEST = (1400, 200, 8, 350)
 
 
 def hbm_peak():
@@ -164,6 +167,69 @@ def cpu_baseline(scene, budget_s: float = 12.0):
 
 # ----------------------------------------------------------------- our arm
 
+def time_substeps(sim, stream, flush, steps: int) -> float:
+    """Device time (ms) of `steps` substeps: CUDA events on the simulation's
+    stream around each substep, L2 flushed between substeps outside them."""
+    import torch
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            starts[k].record(stream)
+            sim.step_async(1)
+            ends[k].record(stream)
+            flush.zero_()
+    sim.synchronize()
+    torch.cuda.synchronize()
+    return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+
+
+def surrogate_leg(args, sim, scenes, stream, flush, plain_ms_per_step: float):
+    """The learned-stress path on the same workload: deformation gradients
+    harvested from a separate plain run of it (snapshots after the impact),
+    network trained on the GPU, held-out stress error against the SVD path,
+    then the same timed loop with the network stress."""
+    from mpm_cuda_b200 import _lib as L
+    from mpm_cuda_b200.surrogate import StressSurrogate
+    from mpm_cuda_b200.train_surrogate import harvest, stress_error
+    solids = [g for s in scenes for g in s.groups if g.material.type in (L.JELLO, L.SNOW)]
+    if scenes[0].dim != 3 or not solids:
+        return {"unavailable": "no 3D jello or snow group in this workload"}
+    fresh, _ = build_workload(args.workload, 0, 1)
+    t0 = time.perf_counter()
+    train_F, held_F = harvest(fresh, start=SURROGATE_HARVEST[0], every=SURROGATE_HARVEST[1],
+                              count=SURROGATE_HARVEST[2], held=SURROGATE_HARVEST[3])
+    rng = np.random.default_rng(0)
+    if train_F.shape[0] > 2_000_000:
+        train_F = train_F[rng.choice(train_F.shape[0], 2_000_000, replace=False)]
+    if held_F.shape[0] > 500_000:
+        held_F = held_F[rng.choice(held_F.shape[0], 500_000, replace=False)]
+    t1 = time.perf_counter()
+    sur = StressSurrogate(device=sim.device)
+    loss = sur.train(train_F)
+    t2 = time.perf_counter()
+    err, accepted = stress_error(sur, held_F, solids[0].material.nu)
+    sim.set_stress_mode(L.STRESS_SURROGATE, sur)
+    sim.step(args.warmup)
+    sim.synchronize()
+    t_ms = time_substeps(sim, stream, flush, args.steps)
+    n_net, n_fb = sim.stress_stats()
+    sim.set_stress_mode(L.STRESS_PLAIN)
+    sur.close()
+    n_part = sum(s.n_particles for s in scenes)
+    ms = t_ms / args.steps
+    return {"value": n_part * args.steps / (t_ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "speedup_vs_plain": plain_ms_per_step / ms,
+            "held_out_stress_error": err, "held_out_accepted": accepted,
+            "network_share_timed": n_net / max(1, n_net + n_fb), "train_loss": loss,
+            "harvest_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 3),
+            "how": "BF16 MLP 10-64-64-9 (SiLU) trained on the GPU from F harvested at substeps "
+                   f"{SURROGATE_HARVEST[0]}+{SURROGATE_HARVEST[1]}k (k=1..{SURROGATE_HARVEST[2]}) of a plain run; "
+                   "error = aggregate relative Kirchhoff stress error vs the SVD path on a later held-out "
+                   "snapshot; timed like the plain line (same K, W, L2 flush)"}
+
+
 def run_ours(args, rank, world, local_rank, dist):
     import ctypes as C
 
@@ -184,23 +250,12 @@ def run_ours(args, rank, world, local_rank, dist):
 
     sim.step(args.warmup)
     sim.synchronize()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     if dist is not None:
         dist.barrier()
-    torch.cuda.synchronize()
     with ClockSampler(local_rank) as clk:
-        with torch.cuda.stream(stream):
-            for k in range(args.steps):
-                starts[k].record(stream)
-                sim.step_async(1)
-                ends[k].record(stream)
-                flush.zero_()
-        sim.synchronize()
-        torch.cuda.synchronize()
+        t_ms = time_substeps(sim, stream, flush, args.steps)
     if dist is not None:
         dist.barrier()
-    t_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     t = torch.tensor([t_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
     n_all = torch.tensor([float(n_part)], dtype=torch.float64, device=f"cuda:{local_rank}")
     if dist is not None:
@@ -258,6 +313,9 @@ def run_ours(args, rank, world, local_rank, dist):
     e2e_t_t = torch.tensor([e2e_t], dtype=torch.float64, device=f"cuda:{local_rank}")
     if dist is not None:
         dist.all_reduce(e2e_t_t, op=dist.ReduceOp.MAX)
+    sur = None
+    if world == 1 and not args.no_surrogate:
+        sur = surrogate_leg(args, sim, scenes, stream, flush, t_max_s * 1e3 / args.steps)
     e2e = {"value": total_particles * e2e_steps / float(e2e_t_t.item()), "unit": UNIT,
            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(n_part * d * 4),
            "how": "mpm_step(h, 1) then mpm_get_positions into page-locked host memory every substep, wall clock "
@@ -274,7 +332,7 @@ def run_ours(args, rank, world, local_rank, dist):
                                          "chosen_by": "autotuner" if args.kernel_config < 0 else "flag"},
                        "l2": "flushed between substeps (256 MB write, outside the timed events)",
                        "parallelism": f"replicas x{world}" if args.workload != "c4" else f"scenes split over {world}"},
-            "roofline": roofline, "e2e": e2e,
+            "roofline": roofline, "e2e": e2e, "surrogate": sur,
             "gpu_launches": launches_per_step * args.steps + 10 * (args.steps // 16 + 1),
             "clocks": clocks}
     return line, scenes
@@ -329,6 +387,7 @@ def main():
     ap.add_argument("--mode", default="binned", choices=["binned", "direct"])
     ap.add_argument("--kernel-config", type=int, default=-1, help="fused-kernel configuration; -1 = autotune")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-stress comparison")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -40,7 +40,9 @@ __device__ __forceinline__ bool make_stencil(const float* x, const SceneParams& 
             st.w[a][k] = ax.w[k];
             st.dw[a][k] = ax.dw[k];
         }
-        if (ax.base < 0 || ax.base + 2 >= sc.n[a]) {
+        // base > n - 3 rather than base + 2 >= n: a huge finite coordinate
+        // converts to INT_MAX, and base + 2 would wrap around
+        if (ax.base < 0 || ax.base > sc.n[a] - 3) {
             err |= ERR_OUT_OF_GRID;
             ok = false;
         }

@@ -137,6 +137,7 @@ class Simulation:
         lib = L.load()
         self.scenes = list(scenes)
         self.dim = self.scenes[0].dim
+        self.device = device
         sdescs, keep = scene_descs(self.scenes)
         opt = L.Options()
         lib.mpm_default_options(C.byref(opt))

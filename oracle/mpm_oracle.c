@@ -218,7 +218,9 @@ void orc_kirchhoff_fcr(int d, const double *F, double mu, double lambda, double 
 }
 
 static int base_index(double x, double o, double h) {
-    int b = (int)((x - o - 0.5 * h) / h); /* C truncation, as MPMCUDA.cu:356 */
+    double q = (x - o - 0.5 * h) / h;
+    if (!(q < 1e9)) q = 1e9; /* far outside: stays out of the grid, no int overflow */
+    int b = (int)q;          /* C truncation, as MPMCUDA.cu:356 */
     return b < 0 ? 0 : b;
 }
 

@@ -157,6 +157,20 @@ def test_out_of_grid_particle_sets_error_word(gpu):
         assert sim.device_errors() == 0
 
 
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
+def test_far_outside_particle_sets_error_word(gpu, mode):
+    # coordinates beyond the int range of node indices: the stencil check
+    # must reject them without overflowing (base saturates to INT_MAX/INT_MIN)
+    sc = blob_scene(3, "jello", seed=73)
+    sc.groups[0].x[0] = np.float32([3e9, 0.5, 0.5])
+    sc.groups[0].x[1] = np.float32([0.5, -3e9, 0.5])
+    with Simulation([sc], p2g_mode=mode) as sim:
+        assert sim.step_status(2) == L.ERR_SIM
+        assert sim.device_errors() & L.DEVERR_OUT_OF_GRID
+        st = sim.get_state(0)
+    assert np.isfinite(st["x"][2:]).all()
+
+
 def test_nan_particle_sets_error_word(gpu):
     sc = blob_scene(3, "jello", seed=71)
     sc.groups[0].x[3, 1] = np.float32(np.nan)
