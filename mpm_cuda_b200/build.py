@@ -5,6 +5,7 @@ The library exports the C ABI declared in ``include/mpm_b200.h``.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -20,7 +21,8 @@ BUILD_DIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "--expt-relaxed-constexpr", "-I", CSRC, "-I", INCLUDE]
-CU_SOURCES = ["mpm_abi.cu", "mpm_engine.cu", "mpm_noalloc.cu", "mpm_surrogate.cu"]
+CU_SOURCES = ["mpm_abi.cu", "mpm_engine.cu", "mpm_fused_plain.cu", "mpm_fused_sur.cu", "mpm_noalloc.cu",
+              "mpm_surrogate.cu"]
 CPP_SOURCES = ["bgeo.cpp"]
 
 
@@ -45,9 +47,9 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         return LIB
     nvcc = _nvcc()
     os.makedirs(BUILD_DIR, exist_ok=True)
-    objs = []
     extra = ["-Xptxas", "-v"] if ptxas_info else []
-    for src in CU_SOURCES + CPP_SOURCES:
+
+    def compile_one(src: str) -> str:
         obj = os.path.join(BUILD_DIR, os.path.splitext(src)[0] + ".o")
         cmd = [nvcc, *ARCH, *NVCC_FLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
         if src.endswith(".cpp"):
@@ -61,7 +63,11 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             sys.stderr.write(r.stderr)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr}")
-        objs.append(obj)
+        return obj
+
+    # the translation units are independent: compile them in parallel
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as pool:
+        objs = list(pool.map(compile_one, CU_SOURCES + CPP_SOURCES))
     tmp = LIB + ".tmp"
     cmd = [nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -1,0 +1,19 @@
+// Kernel tables of the fused substep: the plain and surrogate-stress kernels
+// for a (dimension, material, launch configuration).
+#pragma once
+
+#include "mpm_config.cuh"
+#include "mpm_kernels_binned.cuh"
+#include "mpm_kernels_surrogate.cuh"
+
+namespace mpm {
+
+using FusedFn = void (*)(ParticleBuf, FusedArgs);
+using SurFn = void (*)(ParticleBuf, FusedArgs, SurArgs);
+
+// k_g2p2g<dim, mat, kFusedCfgs[ci]>
+FusedFn fused_fn(int dim, int mat, int ci);
+// k_g2p2g_sur<mat, kFusedCfgs[ci]> (3D jello and snow)
+SurFn sur_fn(int mat, int ci);
+
+}  // namespace mpm

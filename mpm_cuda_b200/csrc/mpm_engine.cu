@@ -15,7 +15,7 @@
 #include "mpm_kernels_binned.cuh"
 #include "mpm_kernels_det.cuh"
 #include "mpm_kernels_direct.cuh"
-#include "mpm_kernels_surrogate.cuh"
+#include "mpm_dispatch.cuh"
 #include "mpm_surrogate.cuh"
 
 namespace mpm {
@@ -73,50 +73,6 @@ __global__ void k_gather_positions(const float* __restrict__ s, const uint32_t* 
 unsigned grid_blocks(long long n, int threads) { return (unsigned)std::max<long long>(1, (n + threads - 1) / threads); }
 
 }  // namespace
-
-// the fused kernel instantiations, indexed [material][config]
-template <int D, int MAT, int CI>
-static constexpr auto fused_kernel() {
-    return &k_g2p2g<D, MAT, kFusedCfgs[CI].chunk, kFusedCfgs[CI].min_ctas, kFusedCfgs[CI].scatter>;
-}
-
-template <int D, int MAT>
-static void (*fused_for(int ci))(ParticleBuf, FusedArgs) {
-    static_assert(kNumFusedCfgs == 8, "update the dispatch table");
-    switch (ci) {
-        case 0: return fused_kernel<D, MAT, 0>();
-        case 1: return fused_kernel<D, MAT, 1>();
-        case 2: return fused_kernel<D, MAT, 2>();
-        case 3: return fused_kernel<D, MAT, 3>();
-        case 4: return fused_kernel<D, MAT, 4>();
-        case 5: return fused_kernel<D, MAT, 5>();
-        case 6: return fused_kernel<D, MAT, 6>();
-        default: return fused_kernel<D, MAT, 7>();
-    }
-}
-
-template <int D>
-static void (*fused_for_mat(int mat, int ci))(ParticleBuf, FusedArgs) {
-    if (mat == JELLO) return fused_for<D, JELLO>(ci);
-    if (mat == SNOW) return fused_for<D, SNOW>(ci);
-    return fused_for<D, WATER>(ci);
-}
-
-static void (*fused_fn(int dim, int mat, int ci))(ParticleBuf, FusedArgs) {
-    return dim == 3 ? fused_for_mat<3>(mat, ci) : fused_for_mat<2>(mat, ci);
-}
-
-// the surrogate kernel closest to a fused-kernel configuration: 64 or 128
-// particles per CTA, at the lower or higher launch-bound occupancy
-template <int MAT>
-static void (*sur_for(const FusedCfg& c))(ParticleBuf, FusedArgs, SurArgs) {
-    if (c.chunk <= 64) return c.min_ctas >= 10 ? &k_g2p2g_sur<MAT, 64, 12> : &k_g2p2g_sur<MAT, 64, 8>;
-    return c.min_ctas >= 6 ? &k_g2p2g_sur<MAT, 128, 6> : &k_g2p2g_sur<MAT, 128, 4>;
-}
-static void (*sur_fn(int mat, int ci))(ParticleBuf, FusedArgs, SurArgs) {
-    return mat == SNOW ? sur_for<SNOW>(kFusedCfgs[ci]) : sur_for<JELLO>(kFusedCfgs[ci]);
-}
-static int sur_chunk(int ci) { return kFusedCfgs[ci].chunk <= 64 ? 64 : 128; }
 
 int Engine::cuda_fail(cudaError_t e, const char* what) {
     char buf[512];
@@ -429,7 +385,7 @@ void Engine::set_config(int ci) {
 void Engine::sur_occupancy() {
     for (int mat = 0; mat < kMats; ++mat) {
         if (!sur_kernel(mat)) continue;
-        const int ch = sur_chunk(cfg);
+        const int ch = kFusedCfgs[cfg].chunk;
         int per_sm = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sur_fn(mat, cfg), ch, 0) != cudaSuccess) {
             cudaGetLastError();
@@ -700,8 +656,7 @@ void Engine::enqueue_g2p2g(int parity) {
         bump = false;
         if (sur_kernel(mat)) {
             const SurArgs SA{&sur->weights->f, sur->meta, sur_counts};
-            const int ch = sur_chunk(cfg);
-            sur_fn(mat, cfg)<<<sur_ctas[mat], ch, 0, stream>>>(buf(parity), A, SA);
+            sur_fn(mat, cfg)<<<sur_ctas[mat], kFusedCfgs[cfg].chunk, 0, stream>>>(buf(parity), A, SA);
             note_launch("k_g2p2g_sur");
         } else {
             fused_fn(dim, mat, cfg)<<<fused_ctas[mat], kFusedCfgs[cfg].chunk, 0, stream>>>(buf(parity), A);

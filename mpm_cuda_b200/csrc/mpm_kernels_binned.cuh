@@ -37,8 +37,7 @@ struct Chunk {
 
 // Tile layout.  3D: window 8^3; the velocity tile (float4) has strides
 // (1, 12, 96) so the 8 lanes of an LDS.128 phase (cells x 0..3, y 0..1) read
-// 8 distinct 16-byte bank groups; the momentum planes (float) have strides
-// (1, 8, 68) so 32 lanes on a 4x4x2 cell patch hit 32 distinct banks.
+// 8 distinct 16-byte bank groups.
 template <int D>
 struct TileShape;
 
@@ -48,7 +47,6 @@ struct TileShape<3> {
     static constexpr int T = 8;
     static constexpr int N = 512;
     static constexpr int VY = 12, VZ = 96, VN = 768;
-    static constexpr int MY = 8, MZ = 68, MN = 7 + 7 * 8 + 7 * 68 + 1;
 };
 
 template <>
@@ -57,7 +55,6 @@ struct TileShape<2> {
     static constexpr int T = 12;
     static constexpr int N = 144;
     static constexpr int VY = 12, VZ = 0, VN = 144;
-    static constexpr int MY = 12, MZ = 0, MN = 144;
 };
 
 // ------------------------------------------------------------- binning --
@@ -117,7 +114,7 @@ __global__ void __launch_bounds__(256) k_bin_gather(ParticleBuf src, ParticleBuf
 
 // one chunk per `chunk` particles of every non-empty (block, material)
 // segment, appended to that material's list
-__global__ void __launch_bounds__(256) k_make_chunks(const int* __restrict__ seg_count,
+static __global__ void __launch_bounds__(256) k_make_chunks(const int* __restrict__ seg_count,
                                                      const int* __restrict__ seg_start, long long n_segs,
                                                      Chunk* __restrict__ chunks, long long list_cap,
                                                      int* __restrict__ n_chunks, int chunk) {
@@ -139,7 +136,7 @@ __global__ void __launch_bounds__(256) k_make_chunks(const int* __restrict__ seg
 }
 
 // zero the cell and segment counters the last k_bin_key touched
-__global__ void __launch_bounds__(256) k_bin_reset(const unsigned long long* __restrict__ keys, long long n,
+static __global__ void __launch_bounds__(256) k_bin_reset(const unsigned long long* __restrict__ keys, long long n,
                                                    int* __restrict__ cell_count, int* __restrict__ seg_count) {
     const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
@@ -149,7 +146,7 @@ __global__ void __launch_bounds__(256) k_bin_reset(const unsigned long long* __r
     seg_count[b * 4 + (int)((k >> 10) & 3)] = 0;
 }
 
-__global__ void k_count_rebin(int* counter) { *counter += 1; }
+static __global__ void k_count_rebin(int* counter) { *counter += 1; }
 
 // ------------------------------------------------------ block activity --
 
@@ -260,11 +257,6 @@ struct FusedArgs {
 template <int D>
 __device__ __forceinline__ int tv_idx(int x, int y, int z) {
     return x + TileShape<D>::VY * y + TileShape<D>::VZ * z;
-}
-
-template <int D>
-__device__ __forceinline__ int tm_idx(int x, int y, int z) {
-    return x + TileShape<D>::MY * y + TileShape<D>::MZ * z;
 }
 
 // ---- pieces of the fused pass (shared by the plain and surrogate kernels)
@@ -415,21 +407,13 @@ __device__ __forceinline__ void mark_touched(unsigned touched, const SceneParams
 // velocity tile, F / Jp / J update, advection, stress, and P2G of the next
 // substep (MPMCUDA.cu:310-741 in one pass: the reference runs P2G, VelUpdate
 // and InterpolateAndMove as three kernels with full-grid sweeps and host
-// syncs between them).  Two scatter variants (SCAT):
-//   0  into a shared momentum window with shared-memory atomics; the 32 lanes
-//      of a warp hit 32 different nodes (sort order) in 32 different banks
-//      (window strides); the window is flushed once with float4 atomics
-//   1  straight to global memory with float4 vector reductions
-//      (red.global.add.v4.f32); no momentum window, so more CTAs fit per SM
-template <int D, int MAT, int CHUNK, int MINB, int SCAT>
+// syncs between them).  The P2G scatter reduces straight to global memory
+// with float4 vector reductions (red.global.add.v4.f32).
+template <int D, int MAT, int CHUNK, int MINB>
 __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs A) {
     using P = Planes<D>;
     using TS = TileShape<D>;
-    constexpr int T = TS::T;
-    constexpr int TN = TS::N;
-    constexpr int MN = SCAT == 0 ? TS::MN : 1;
     __shared__ float4 tv[TS::VN];  // grid velocity window
-    __shared__ float tm[4][MN];    // next-substep momentum / mass window (SCAT 0)
     __shared__ unsigned touched;   // 3^D neighbour-block bits
     __shared__ int s_chunk;
 
@@ -448,22 +432,12 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
         tile_origin<D>(sc, ch.block - sc.block_off, o);
         if (threadIdx.x == 0) touched = 0u;
         load_velocity_tile<D, CHUNK>(sc, o, A.grid_vel, tv);
-        if (SCAT == 0) {
-            for (int t = threadIdx.x; t < TN; t += CHUNK) {
-                const int m = tm_idx<D>(t % T, (t / T) % T, (D == 3) ? t / (T * T) : 0);
-                tm[0][m] = 0.f;
-                tm[1][m] = 0.f;
-                tm[2][m] = 0.f;
-                tm[3][m] = 0.f;
-            }
-        }
         __syncthreads();
 
         if ((int)threadIdx.x < ch.count) {
             const long long i = (long long)ch.start + threadIdx.x;
             float* S = pb.s;
             const long long cap = pb.cap;
-            const GroupParams g = A.groups[pb.grp[i]];
             unsigned err = 0;
             float x[D];
 #pragma unroll
@@ -472,6 +446,8 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
             if (make_stencil<D>(x, sc, st, err)) {
                 G2PAcc<D> acc;
                 g2p_window<D>(st, o, tv, sc, A, acc);
+                // loaded after the gather, its register peak
+                const GroupParams g = A.groups[pb.grp[i]];
                 float F[D * D], Cn[D * D], v[D], aux;
                 err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux);
 
@@ -480,43 +456,12 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
                 if (make_stencil<D>(x, sc, sn, err)) {
                     P2GSource<D> src;
                     particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc, src);
-                    if (SCAT == 0) {
-                        if (in_window<D>(sn.base, o)) {
-                            const int l0 = sn.base[0] - o[0], l1 = sn.base[1] - o[1],
-                                      l2 = D == 3 ? sn.base[2] - o[2] : 0;
-                            p2g_scatter<D>(sn, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 cc) {
-                                const int m = tm_idx<D>(l0 + ox, l1 + oy, l2 + oz);
-                                atomicAdd(&tm[0][m], cc.x);
-                                atomicAdd(&tm[1][m], cc.y);
-                                if (D == 3) atomicAdd(&tm[2][m], cc.z);
-                                atomicAdd(&tm[3][m], cc.w);
-                            });
-                            atomicOr(&touched, touched_bits<D>(l0, l1, l2));
-                        } else {
-                            atomicAdd(A.fallback, 1u);
-                            p2g_global<D>(sn, src, sc, A.grid_mom, A.blk_flag, A.active, A.n_active);
-                        }
-                    } else {
-                        scatter_global<D>(sn, src, sc, o, A, &touched);
-                    }
+                    scatter_global<D>(sn, src, sc, o, A, &touched);
                 }
             }
             if (err) atomicOr(A.err_word, err);
         }
         __syncthreads();
-
-        // ---- flush the momentum window (SCAT 0) and mark touched blocks
-        if (SCAT == 0) {
-            for (int t = threadIdx.x; t < TN; t += CHUNK) {
-                const int tx = t % T, ty = (t / T) % T, tz = (D == 3) ? t / (T * T) : 0;
-                const int m = tm_idx<D>(tx, ty, tz);
-                const float mm = tm[3][m];
-                const float mx = tm[0][m], my = tm[1][m], mz = tm[2][m];
-                if (mm != 0.f || mx != 0.f || my != 0.f || mz != 0.f)
-                    atomicAdd(&A.grid_mom[node_index<D>(sc, o[0] + tx, o[1] + ty, o[2] + tz)],
-                              make_float4(mx, my, mz, mm));
-            }
-        }
         mark_touched<D>(touched, sc, o, A);
         __syncthreads();
     }

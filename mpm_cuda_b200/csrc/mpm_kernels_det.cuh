@@ -95,17 +95,6 @@ __global__ void __launch_bounds__(256) k_det_reset(const unsigned long long* __r
     cell_end[k] = 0;
 }
 
-// weights of the three stencil nodes of one axis from the base fraction fx
-__device__ __forceinline__ void weights_from_fx(float fx, float* w, float* dw) {
-    const float t0 = 1.5f - fx, t1 = fx - 1.f, t2 = fx - 0.5f;
-    w[0] = 0.5f * t0 * t0;
-    w[1] = 0.75f - t1 * t1;
-    w[2] = 0.5f * t2 * t2;
-    dw[0] = -t0;
-    dw[1] = -2.f * t1;
-    dw[2] = t2;
-}
-
 // Every node of the active blocks sums the records of the base nodes
 // node - o, o in {0,1,2}^D, in the order (o, sorted position), and stores it.
 template <int D>
@@ -144,7 +133,6 @@ __global__ void __launch_bounds__(256) k_det_gather(const float* __restrict__ sr
 #pragma unroll
                         for (int a = 0; a < D; ++a) {
                             st.fx[a] = src[(SP::FX + a) * cap + p];
-                            weights_from_fx(st.fx[a], st.w[a], st.dw[a]);
                             s.mv[a] = src[(SP::MV + a) * cap + p];
                         }
 #pragma unroll

@@ -244,24 +244,72 @@ MPM_HD void svd(const float* F, float* U, float* s, float* V) {
 // R = U V^T, J = det F.  With F = U S V^T, (F - R) F^T = U (S^2 - S) U^T, so
 // only U and s are needed:  tau = U diag(2 mu s_i (s_i - 1)) U^T
 //                                 + lambda J (J - 1) I.
-template <int D>
-MPM_HD void kirchhoff_fcr(const float* F, float mu, float lambda, float* tau) {
-    float U[D * D], s[D], V[D * D];
-    svd<D>(F, U, s, V);
-    const float J = det<D>(F);
+//
+// In 3D the left singular vectors and singular values come from the
+// eigendecomposition of B = F F^T = U diag(s^2) U^T (the same 4 cyclic Jacobi
+// sweeps as svd3, accumulating U instead of V), so V, its polish and the
+// Gram-Schmidt step are not needed: s_i = sqrt(eig_i), and when det F < 0 the
+// smallest one is negated (the convention of the SVD: s0 >= s1 >= |s2|, the
+// last carrying the sign of det F).  The sum over k does not depend on the
+// order of the eigenpairs, so they are not sorted.
+MPM_HD void kirchhoff_fcr3(const float* F, float mu, float lambda, float* tau) {
+    float S[9], U[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            S[i * 3 + j] = F[i * 3 + 0] * F[j * 3 + 0] + F[i * 3 + 1] * F[j * 3 + 1] + F[i * 3 + 2] * F[j * 3 + 2];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) U[i] = (i % 4 == 0) ? 1.f : 0.f;
+#pragma unroll
+    for (int sweep = 0; sweep < 4; ++sweep) {
+        jacobi_rotate<0, 1>(S, U);
+        jacobi_rotate<0, 2>(S, U);
+        jacobi_rotate<1, 2>(S, U);
+    }
+    const float J = det<3>(F);
+    float s[3] = {sqrtf(fmaxf(S[0], 0.f)), sqrtf(fmaxf(S[4], 0.f)), sqrtf(fmaxf(S[8], 0.f))};
+    if (J < 0.f) {
+        const int k = (S[0] <= S[4] && S[0] <= S[8]) ? 0 : (S[4] <= S[8] ? 1 : 2);
+        s[k] = -s[k];
+    }
     const float iso = lambda * J * (J - 1.f);
-    float dg[D];
+    float dg[3];
 #pragma unroll
-    for (int k = 0; k < D; ++k) dg[k] = 2.f * mu * s[k] * (s[k] - 1.f);
+    for (int k = 0; k < 3; ++k) dg[k] = 2.f * mu * s[k] * (s[k] - 1.f);
 #pragma unroll
-    for (int i = 0; i < D; ++i)
+    for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < D; ++j) {
+        for (int j = 0; j < 3; ++j) {
             float acc = (i == j) ? iso : 0.f;
 #pragma unroll
-            for (int k = 0; k < D; ++k) acc = fmaf(U[i * D + k] * dg[k], U[j * D + k], acc);
-            tau[i * D + j] = acc;
+            for (int k = 0; k < 3; ++k) acc = fmaf(U[i * 3 + k] * dg[k], U[j * 3 + k], acc);
+            tau[i * 3 + j] = acc;
         }
+}
+
+template <int D>
+MPM_HD void kirchhoff_fcr(const float* F, float mu, float lambda, float* tau) {
+    if constexpr (D == 3) {
+        kirchhoff_fcr3(F, mu, lambda, tau);
+    } else {
+        float U[4], s[2], V[4];
+        svd2(F, U, s, V);
+        const float J = det<2>(F);
+        const float iso = lambda * J * (J - 1.f);
+        float dg[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) dg[k] = 2.f * mu * s[k] * (s[k] - 1.f);
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                float acc = (i == j) ? iso : 0.f;
+#pragma unroll
+                for (int k = 0; k < 2; ++k) acc = fmaf(U[i * 2 + k] * dg[k], U[j * 2 + k], acc);
+                tau[i * 2 + j] = acc;
+            }
+    }
 }
 
 // ------------------------------------------------------------- B-spline --

@@ -12,8 +12,28 @@ template <int D>
 struct Stencil {
     int base[3];
     float fx[3];
-    float w[3][3];
-    float dw[3][3];
+    // quadratic B-spline weight and derivative (d/dx in cell units) of node
+    // base + k along axis a, recomputed from fx where used (the same
+    // arithmetic as axis_weights) instead of held in 18 registers
+    __device__ __forceinline__ float w(int a, int k) const {
+        const float f = fx[a];
+        if (k == 0) {
+            const float t0 = 1.5f - f;
+            return 0.5f * t0 * t0;
+        }
+        if (k == 1) {
+            const float t1 = f - 1.f;
+            return 0.75f - t1 * t1;
+        }
+        const float t2 = f - 0.5f;
+        return 0.5f * t2 * t2;
+    }
+    __device__ __forceinline__ float dw(int a, int k) const {
+        const float f = fx[a];
+        if (k == 0) return -(1.5f - f);
+        if (k == 1) return -2.f * (f - 1.f);
+        return f - 0.5f;
+    }
 };
 
 // Returns false (and sets error bits) when the 3^D stencil leaves the grid
@@ -35,11 +55,6 @@ __device__ __forceinline__ bool make_stencil(const float* x, const SceneParams& 
         Axis ax = axis_weights(gx);
         st.base[a] = ax.base;
         st.fx[a] = ax.fx;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            st.w[a][k] = ax.w[k];
-            st.dw[a][k] = ax.dw[k];
-        }
         // base > n - 3 rather than base + 2 >= n: a huge finite coordinate
         // converts to INT_MAX, and base + 2 would wrap around
         if (ax.base < 0 || ax.base > sc.n[a] - 3) {
@@ -123,8 +138,8 @@ __device__ __forceinline__ float4 p2g_node(const Stencil<D>& st, const P2GSource
     float wa[3], dwa[3];
 #pragma unroll
     for (int a = 0; a < D; ++a) {
-        wa[a] = st.w[a][o[a]];
-        dwa[a] = st.dw[a][o[a]];
+        wa[a] = st.w(a, o[a]);
+        dwa[a] = st.dw(a, o[a]);
     }
     float w = wa[0] * wa[1];
     float gw[D];
@@ -179,8 +194,8 @@ __device__ __forceinline__ void g2p_node(const Stencil<D>& st, const int* o, flo
     float wa[3], dwa[3];
 #pragma unroll
     for (int a = 0; a < D; ++a) {
-        wa[a] = st.w[a][o[a]];
-        dwa[a] = st.dw[a][o[a]];
+        wa[a] = st.w(a, o[a]);
+        dwa[a] = st.dw(a, o[a]);
     }
     float w = wa[0] * wa[1];
     float gw[D];
@@ -237,14 +252,17 @@ __device__ __forceinline__ void g2p_gather(const Stencil<D>& st, float inv_h, Fe
         for (int ox = 0; ox < 3; ++ox) {
             float B00[3] = {0.f, 0.f, 0.f}, B10[3] = {0.f, 0.f, 0.f}, B20[3] = {0.f, 0.f, 0.f};
             float B01[3] = {0.f, 0.f, 0.f}, B02[3] = {0.f, 0.f, 0.f};
-#pragma unroll
+            // the y loop stays rolled: fully unrolled, the 27 hoisted tile
+            // loads and the partial sums exceed the register budget of the
+            // high-occupancy launch configurations and spill
+#pragma unroll 1
             for (int oy = 0; oy < 3; ++oy) {
                 float A0[3] = {0.f, 0.f, 0.f}, A1[3] = {0.f, 0.f, 0.f}, A2[3] = {0.f, 0.f, 0.f};
 #pragma unroll
                 for (int oz = 0; oz < 3; ++oz) {
                     const float4 g = fetch(ox, oy, oz);
                     const float vi[3] = {g.x, g.y, g.z};
-                    const float wz = st.w[2][oz], dz = st.dw[2][oz];
+                    const float wz = st.w(2, oz), dz = st.dw(2, oz);
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         A0[c] = fmaf(wz, vi[c], A0[c]);
@@ -252,7 +270,7 @@ __device__ __forceinline__ void g2p_gather(const Stencil<D>& st, float inv_h, Fe
                         A2[c] = fmaf(dz, vi[c], A2[c]);
                     }
                 }
-                const float wy = st.w[1][oy], dy = st.dw[1][oy], wyo = (float)oy * wy;
+                const float wy = st.w(1, oy), dy = st.dw(1, oy), wyo = (float)oy * wy;
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
                     B00[c] = fmaf(wy, A0[c], B00[c]);
@@ -262,7 +280,7 @@ __device__ __forceinline__ void g2p_gather(const Stencil<D>& st, float inv_h, Fe
                     B02[c] = fmaf(wy, A2[c], B02[c]);
                 }
             }
-            const float wx = st.w[0][ox], dx = st.dw[0][ox], wxo = (float)ox * wx;
+            const float wx = st.w(0, ox), dx = st.dw(0, ox), wxo = (float)ox * wx;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 v[c] = fmaf(wx, B00[c], v[c]);
@@ -282,7 +300,7 @@ __device__ __forceinline__ void g2p_gather(const Stencil<D>& st, float inv_h, Fe
             for (int oy = 0; oy < 3; ++oy) {
                 const float4 g = fetch(ox, oy, 0);
                 const float vi[2] = {g.x, g.y};
-                const float wy = st.w[1][oy], dy = st.dw[1][oy];
+                const float wy = st.w(1, oy), dy = st.dw(1, oy);
 #pragma unroll
                 for (int c = 0; c < 2; ++c) {
                     A0[c] = fmaf(wy, vi[c], A0[c]);
@@ -290,7 +308,7 @@ __device__ __forceinline__ void g2p_gather(const Stencil<D>& st, float inv_h, Fe
                     A2[c] = fmaf(dy, vi[c], A2[c]);
                 }
             }
-            const float wx = st.w[0][ox], dx = st.dw[0][ox], wxo = (float)ox * wx;
+            const float wx = st.w(0, ox), dx = st.dw(0, ox), wxo = (float)ox * wx;
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
                 v[c] = fmaf(wx, A0[c], v[c]);
@@ -337,8 +355,8 @@ __device__ __forceinline__ void p2g_scatter(const Stencil<D>& st, const P2GSourc
         for (int ox = 0; ox < 3; ++ox)
 #pragma unroll
             for (int oy = 0; oy < 3; ++oy) {
-                const float wx = st.w[0][ox], wy = st.w[1][oy];
-                const float P = wx * wy, Qx = st.dw[0][ox] * wy, Qy = wx * st.dw[1][oy];
+                const float wx = st.w(0, ox), wy = st.w(1, oy);
+                const float P = wx * wy, Qx = st.dw(0, ox) * wy, Qy = wx * st.dw(1, oy);
                 float lin[3], K[3];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
@@ -347,8 +365,8 @@ __device__ __forceinline__ void p2g_scatter(const Stencil<D>& st, const P2GSourc
                 }
 #pragma unroll
                 for (int oz = 0; oz < 3; ++oz) {
-                    const float wz = st.w[2][oz];
-                    const float w = P * wz, Pdz = P * st.dw[2][oz];
+                    const float wz = st.w(2, oz);
+                    const float w = P * wz, Pdz = P * st.dw(2, oz);
                     float out[3];
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
@@ -361,14 +379,14 @@ __device__ __forceinline__ void p2g_scatter(const Stencil<D>& st, const P2GSourc
     } else {
 #pragma unroll
         for (int ox = 0; ox < 3; ++ox) {
-            const float wx = st.w[0][ox], dx = st.dw[0][ox];
+            const float wx = st.w(0, ox), dx = st.dw(0, ox);
             float lin[2];
 #pragma unroll
             for (int c = 0; c < 2; ++c) lin[c] = fmaf(beta[c][0], (float)ox, alpha[c]);
 #pragma unroll
             for (int oy = 0; oy < 3; ++oy) {
-                const float wy = st.w[1][oy];
-                const float w = wx * wy, gx = dx * wy, gy = wx * st.dw[1][oy];
+                const float wy = st.w(1, oy);
+                const float w = wx * wy, gx = dx * wy, gy = wx * st.dw(1, oy);
                 float out[2];
 #pragma unroll
                 for (int c = 0; c < 2; ++c) {
