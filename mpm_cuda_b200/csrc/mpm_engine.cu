@@ -387,7 +387,13 @@ void Engine::sur_occupancy() {
         if (!sur_kernel(mat)) continue;
         const int ch = kFusedCfgs[cfg].chunk;
         int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sur_fn(mat, cfg), ch, 0) != cudaSuccess) {
+        // the network rows live in dynamic shared memory; with the windows and
+        // weights they can exceed the 48 KB a kernel gets without opting in
+        if (cudaFuncSetAttribute(sur_fn(mat, cfg), cudaFuncAttributeMaxDynamicSharedMemorySize, sur_dyn_smem(ch)) !=
+            cudaSuccess)
+            cudaGetLastError();  // not fatal here: the occupancy query and the launch report it
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sur_fn(mat, cfg), ch, sur_dyn_smem(ch)) !=
+            cudaSuccess) {
             cudaGetLastError();
             per_sm = 1;
         }
@@ -656,7 +662,8 @@ void Engine::enqueue_g2p2g(int parity) {
         bump = false;
         if (sur_kernel(mat)) {
             const SurArgs SA{&sur->weights->f, sur->meta, sur_counts};
-            sur_fn(mat, cfg)<<<sur_ctas[mat], kFusedCfgs[cfg].chunk, 0, stream>>>(buf(parity), A, SA);
+            const int ch = kFusedCfgs[cfg].chunk;
+            sur_fn(mat, cfg)<<<sur_ctas[mat], ch, sur_dyn_smem(ch), stream>>>(buf(parity), A, SA);
             note_launch("k_g2p2g_sur");
         } else {
             fused_fn(dim, mat, cfg)<<<fused_ctas[mat], kFusedCfgs[cfg].chunk, 0, stream>>>(buf(parity), A);

@@ -270,17 +270,35 @@ __device__ __forceinline__ void tile_origin(const SceneParams& sc, long long lb,
     o[2] = (D == 3) ? (int)(lb / ((long long)sc.nb[0] * sc.nb[1])) * SIDE - 1 : 0;
 }
 
-// grid velocity window of a chunk (zero outside the grid), NT threads
+// 16-byte asynchronous global -> shared copy (cp.async.cg), zero-filled
+// when `valid` is false (source size 0: nothing is read)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// starts the asynchronous copy of chunk c's grid-velocity window into tv
+// (zero outside the grid), NT threads
 template <int D, int NT>
-__device__ __forceinline__ void load_velocity_tile(const SceneParams& sc, const int* o, const float4* __restrict__ grid_vel,
-                                                   float4* tv) {
+__device__ __forceinline__ void prefetch_velocity_tile(const FusedArgs& A, int c, float4* tv) {
     constexpr int T = TileShape<D>::T;
+    const Chunk ch = A.chunks[c];
+    const SceneParams& sc = A.scenes[scene_of_block(A.scenes, A.n_scenes, ch.block)];
+    int o[3];
+    tile_origin<D>(sc, ch.block - sc.block_off, o);
     for (int t = threadIdx.x; t < TileShape<D>::N; t += NT) {
         const int tx = t % T, ty = (t / T) % T, tz = (D == 3) ? t / (T * T) : 0;
         const int ix = o[0] + tx, iy = o[1] + ty, iz = o[2] + tz;
         bool in = ix >= 0 && iy >= 0 && ix < sc.n[0] && iy < sc.n[1];
         if (D == 3) in = in && iz >= 0 && iz < sc.n[2];
-        tv[tv_idx<D>(tx, ty, tz)] = in ? grid_vel[node_index<D>(sc, ix, iy, iz)] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4* src = in ? A.grid_vel + node_index<D>(sc, ix, iy, iz) : A.grid_vel;
+        cp_async16(&tv[tv_idx<D>(tx, ty, tz)], src, in);
     }
 }
 
@@ -403,6 +421,54 @@ __device__ __forceinline__ void mark_touched(unsigned touched, const SceneParams
     }
 }
 
+// Persistent loop of a CTA over a material's chunk list.  Chunks come from a
+// global cursor (chunk sizes vary); the index of the chunk after next and the
+// next chunk's velocity window are fetched while the current chunk is
+// processed, so the cursor atomic and the window's L2 round trips are off the
+// critical path.  body(ch, sc, o, tv, touched) runs with chunk ch's window in
+// tv; every thread of the CTA calls it.  Three barriers per chunk: window
+// landed, body done (touched complete, window free), loop state published.
+template <int D, int NT, class Body>
+__device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][TileShape<D>::VN],
+                                           unsigned (&touched)[2], int (&s_cn)[2], Body body) {
+    const int nch = *A.n_chunks;
+    if (threadIdx.x == 0) {
+        s_cn[0] = atomicAdd(A.cursor, 1);
+        s_cn[1] = atomicAdd(A.cursor, 1);
+    }
+    __syncthreads();
+    int cur = s_cn[0], nxt = s_cn[1];
+    if (cur < nch) prefetch_velocity_tile<D, NT>(A, cur, tv[0]);
+    cp_async_commit();
+    for (int k = 0; cur < nch; ++k) {
+        const int b = k & 1;
+        if (nxt < nch) prefetch_velocity_tile<D, NT>(A, nxt, tv[b ^ 1]);
+        cp_async_commit();
+        int after = 0;
+        if (threadIdx.x == 0) {
+            after = atomicAdd(A.cursor, 1);
+            touched[b] = 0u;
+        }
+        cp_async_wait<1>();  // this thread's copies of the current window
+        __syncthreads();     // everyone's
+        const Chunk ch = A.chunks[cur];
+        const SceneParams& sc = A.scenes[scene_of_block(A.scenes, A.n_scenes, ch.block)];
+        int o[3];
+        tile_origin<D>(sc, ch.block - sc.block_off, o);
+        body(ch, sc, o, tv[b], &touched[b]);
+        __syncthreads();
+        mark_touched<D>(touched[b], sc, o, A);
+        if (threadIdx.x == 0) {
+            s_cn[0] = nxt;
+            s_cn[1] = after;
+        }
+        __syncthreads();
+        cur = s_cn[0];
+        nxt = s_cn[1];
+    }
+    cp_async_wait<0>();
+}
+
 // One substep for the particles of each chunk of material MAT: G2P from the
 // velocity tile, F / Jp / J update, advection, stress, and P2G of the next
 // substep (MPMCUDA.cu:310-741 in one pass: the reference runs P2G, VelUpdate
@@ -413,58 +479,40 @@ template <int D, int MAT, int CHUNK, int MINB>
 __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs A) {
     using P = Planes<D>;
     using TS = TileShape<D>;
-    __shared__ float4 tv[TS::VN];  // grid velocity window
-    __shared__ unsigned touched;   // 3^D neighbour-block bits
-    __shared__ int s_chunk;
+    __shared__ __align__(16) float4 tv[2][TS::VN];  // grid velocity windows (double-buffered)
+    __shared__ unsigned touched[2];                 // 3^D neighbour-block bits
+    __shared__ int s_cn[2];
 
     if (A.bump_epoch && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.epoch, 1);
-    const int nch = *A.n_chunks;
-    // persistent CTAs take chunks from a global cursor (chunk sizes vary)
-    for (;;) {
-        if (threadIdx.x == 0) s_chunk = atomicAdd(A.cursor, 1);
-        __syncthreads();
-        const int c = s_chunk;
-        if (c >= nch) break;
-        const Chunk ch = A.chunks[c];
-        const int s = scene_of_block(A.scenes, A.n_scenes, ch.block);
-        const SceneParams& sc = A.scenes[s];
-        int o[3];
-        tile_origin<D>(sc, ch.block - sc.block_off, o);
-        if (threadIdx.x == 0) touched = 0u;
-        load_velocity_tile<D, CHUNK>(sc, o, A.grid_vel, tv);
-        __syncthreads();
-
-        if ((int)threadIdx.x < ch.count) {
-            const long long i = (long long)ch.start + threadIdx.x;
-            float* S = pb.s;
-            const long long cap = pb.cap;
-            unsigned err = 0;
-            float x[D];
+    chunk_loop<D, CHUNK>(A, tv, touched, s_cn,
+                         [&](const Chunk& ch, const SceneParams& sc, const int* o, const float4* w, unsigned* tb) {
+        if ((int)threadIdx.x >= ch.count) return;
+        const long long i = (long long)ch.start + threadIdx.x;
+        float* S = pb.s;
+        const long long cap = pb.cap;
+        unsigned err = 0;
+        float x[D];
 #pragma unroll
-            for (int a = 0; a < D; ++a) x[a] = S[(P::X + a) * cap + i];
-            Stencil<D> st;
-            if (make_stencil<D>(x, sc, st, err)) {
-                G2PAcc<D> acc;
-                g2p_window<D>(st, o, tv, sc, A, acc);
-                // loaded after the gather, its register peak
-                const GroupParams g = A.groups[pb.grp[i]];
-                float F[D * D], Cn[D * D], v[D], aux;
-                err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux);
+        for (int a = 0; a < D; ++a) x[a] = S[(P::X + a) * cap + i];
+        Stencil<D> st;
+        if (make_stencil<D>(x, sc, st, err)) {
+            G2PAcc<D> acc;
+            g2p_window<D>(st, o, w, sc, A, acc);
+            // loaded after the gather, its register peak
+            const GroupParams g = A.groups[pb.grp[i]];
+            float F[D * D], Cn[D * D], v[D], aux;
+            err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux);
 
-                // ---- stress + P2G of the next substep
-                Stencil<D> sn;
-                if (make_stencil<D>(x, sc, sn, err)) {
-                    P2GSource<D> src;
-                    particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc, src);
-                    scatter_global<D>(sn, src, sc, o, A, &touched);
-                }
+            // ---- stress + P2G of the next substep
+            Stencil<D> sn;
+            if (make_stencil<D>(x, sc, sn, err)) {
+                P2GSource<D> src;
+                particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc, src);
+                scatter_global<D>(sn, src, sc, o, A, tb);
             }
-            if (err) atomicOr(A.err_word, err);
         }
-        __syncthreads();
-        mark_touched<D>(touched, sc, o, A);
-        __syncthreads();
-    }
+        if (err) atomicOr(A.err_word, err);
+    });
 }
 
 }  // namespace mpm

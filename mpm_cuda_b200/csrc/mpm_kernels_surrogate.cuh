@@ -17,6 +17,12 @@
 
 namespace mpm {
 
+// row stride (floats) of the per-particle network rows in shared memory: odd,
+// so the rows of a warp's 32 particles start in 32 different banks
+constexpr int kSurRowStride = mlp::IN_PAD + 1;
+// dynamic shared memory of k_g2p2g_sur for a chunk size
+constexpr int sur_dyn_smem(int chunk) { return chunk * kSurRowStride * (int)sizeof(float); }
+
 struct SurArgs {
     const mlp::Forward* weights;
     mlp::Meta meta;
@@ -30,36 +36,23 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
     using TS = TileShape<D>;
     static_assert(CHUNK % 32 == 0, "whole warps");
     static_assert(MAT == JELLO || MAT == SNOW, "elastic materials only");
-    __shared__ float4 tv[TS::VN];                      // grid velocity window
-    __shared__ __align__(16) mlp::Forward W;           // network weights
-    constexpr int XS = mlp::IN_PAD + 1;  // odd row stride: per-particle rows hit 32 banks
-    __shared__ float sxy[CHUNK * XS];     // network inputs, then outputs
-    __shared__ unsigned touched;
-    __shared__ int s_chunk;
+    constexpr int XS = kSurRowStride;
+    __shared__ __align__(16) float4 tv[2][TS::VN];  // grid velocity windows (double-buffered)
+    __shared__ __align__(16) mlp::Forward W;        // network weights
+    extern __shared__ float sxy[];                  // CHUNK rows: network inputs, then outputs
+    __shared__ unsigned touched[2];
+    __shared__ int s_cn[2];
 
     if (A.bump_epoch && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.epoch, 1);
     {
         const int4* src = reinterpret_cast<const int4*>(SA.weights);
         int4* dst = reinterpret_cast<int4*>(&W);
         for (int k = threadIdx.x; k < (int)(sizeof(mlp::Forward) / 16); k += CHUNK) dst[k] = src[k];
-    }
+    }  // published by the first barrier of chunk_loop
     const int lane = threadIdx.x & 31, w0 = threadIdx.x & ~31;
     unsigned n_net = 0, n_svd = 0;
-    const int nch = *A.n_chunks;
-    for (;;) {
-        if (threadIdx.x == 0) s_chunk = atomicAdd(A.cursor, 1);
-        __syncthreads();  // also publishes W on the first pass
-        const int c = s_chunk;
-        if (c >= nch) break;
-        const Chunk ch = A.chunks[c];
-        const int s = scene_of_block(A.scenes, A.n_scenes, ch.block);
-        const SceneParams& sc = A.scenes[s];
-        int o[3];
-        tile_origin<D>(sc, ch.block - sc.block_off, o);
-        if (threadIdx.x == 0) touched = 0u;
-        load_velocity_tile<D, CHUNK>(sc, o, A.grid_vel, tv);
-        __syncthreads();
-
+    chunk_loop<D, CHUNK>(A, tv, touched, s_cn,
+                         [&](const Chunk& ch, const SceneParams& sc, const int* o, const float4* w, unsigned* tb) {
         const long long i = (long long)ch.start + threadIdx.x;
         float* S = pb.s;
         const long long cap = pb.cap;
@@ -70,14 +63,14 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
         float* row = sxy + threadIdx.x * XS;
         if ((int)threadIdx.x < ch.count) {
             gi = pb.grp[i];
-            const GroupParams g = A.groups[gi];
             float x[D];
 #pragma unroll
             for (int a = 0; a < D; ++a) x[a] = S[(P::X + a) * cap + i];
             Stencil<D> st;
             if (make_stencil<D>(x, sc, st, err)) {
                 G2PAcc<D> acc;
-                g2p_window<D>(st, o, tv, sc, A, acc);
+                g2p_window<D>(st, o, w, sc, A, acc);
+                const GroupParams g = A.groups[gi];
                 float F[D * D], Cn[D * D], v[D], aux;
                 err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux);
                 Stencil<D> sn;
@@ -113,7 +106,7 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
             if (MAT == SNOW) aux = __ldcg(S + P::AUX * cap + i);
             const GroupParams g = A.groups[gi];
             Stencil<D> sn;
-            make_stencil<D>(x, sc, sn, err);  // the stencil found in phase 1
+            make_stencil<D>(x, sc, sn, err);  // the stencil found above
             float tau[D * D];
             bool use = false;
             if (eligible) {
@@ -135,13 +128,10 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
                 particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc, src);
                 ++n_svd;
             }
-            scatter_global<D>(sn, src, sc, o, A, &touched);
+            scatter_global<D>(sn, src, sc, o, A, tb);
         }
         if (err) atomicOr(A.err_word, err);
-        __syncthreads();
-        mark_touched<D>(touched, sc, o, A);
-        __syncthreads();
-    }
+    });
     n_net = __reduce_add_sync(0xffffffffu, n_net);
     n_svd = __reduce_add_sync(0xffffffffu, n_svd);
     if (lane == 0 && (n_net | n_svd)) {
