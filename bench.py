@@ -114,18 +114,32 @@ class ClockSampler:
 
 def build_workload(name: str, rank: int, world: int):
     from mpm_cuda_b200 import scenes as S
+    from mpm_cuda_b200.ranks import replica_seed, shard
+    seed = replica_seed(1234, rank)
     if name == "c4":
-        all_scenes = S.c4_batched()
-        return [s for i, s in enumerate(all_scenes) if i % world == rank], "c4 64 batched scenes (jello/snow/water)"
+        return shard(S.c4_batched(), rank, world), "c4 64 batched scenes (jello/snow/water)"
     if name == "c0":
-        return [S.c0_jello2d(seed=1234 + rank)], "c0 2D jello 128^2, 9000 particles"
+        return [S.c0_jello2d(seed=seed)], "c0 2D jello 128^2, 9000 particles"
     if name == "c2":
-        return [S.c2_snow3d(seed=1234 + rank)], "c2 3D snow 256^3, two spheres r=0.12, 8 ppc"
+        return [S.c2_snow3d(seed=seed)], "c2 3D snow 256^3, two spheres r=0.12, 8 ppc"
     if name == "c3":
-        return [S.c3_jello3d(seed=1234 + rank)], "c3 3D jello 256^3, 0.245 cube, 8 ppc"
+        return [S.c3_jello3d(seed=seed)], "c3 3D jello 256^3, 0.245 cube, 8 ppc"
     if name == "c3big":
-        return [S.c3_jello3d(seed=1234 + rank, edge=0.45)], "c3 3D jello 256^3, 0.45 cube, 8 ppc"
-    return [S.c1_jello3d(seed=1234 + rank)], "c1 3D jello 128^3, 0.3 cube, 8 ppc"
+        return [S.c3_jello3d(seed=seed, edge=0.45)], "c3 3D jello 256^3, 0.45 cube, 8 ppc"
+    return [S.c1_jello3d(seed=seed)], "c1 3D jello 128^3, 0.3 cube, 8 ppc"
+
+
+def measured_traffic(workload: str, kernel: str):
+    """DRAM bytes per launch of `kernel` on `workload` from the committed ncu
+    summaries (profiles/dram_traffic.txt), or None without a capture."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        f = line.split()
+        if len(f) >= 3 and not line.startswith("#") and f[0] == workload and f[1] == kernel:
+            return int(f[2])
+    return None
 
 
 def state_bytes_per_particle(scenes):
@@ -236,6 +250,7 @@ def run_ours(args, rank, world, local_rank, dist):
     import torch
     from mpm_cuda_b200.sim import Simulation
 
+    from mpm_cuda_b200.ranks import reduce_max, reduce_max_sum
     torch.cuda.set_device(local_rank)
     scenes, desc = build_workload(args.workload, rank, world)
     n_part = sum(s.n_particles for s in scenes)
@@ -256,13 +271,8 @@ def run_ours(args, rank, world, local_rank, dist):
         t_ms = time_substeps(sim, stream, flush, args.steps)
     if dist is not None:
         dist.barrier()
-    t = torch.tensor([t_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-    n_all = torch.tensor([float(n_part)], dtype=torch.float64, device=f"cuda:{local_rank}")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(n_all, op=dist.ReduceOp.SUM)
-    t_max_s = float(t.item()) / 1e3
-    total_particles = float(n_all.item())
+    t_max_ms, total_particles = reduce_max_sum(dist, t_ms, n_part, device=f"cuda:{local_rank}")
+    t_max_s = t_max_ms / 1e3
     value = total_particles * args.steps / t_max_s
     clocks = clk.summary()
 
@@ -291,7 +301,9 @@ def run_ours(args, rank, world, local_rank, dist):
     peak, peak_kind = hbm_peak()
     achieved = alg[dom_name] / (dom_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": peak,
-                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": measured_traffic(args.workload, dom_name) if args.mode == "binned" else None,
+                "traffic_source": "profiles/dram_traffic.txt (ncu dram__bytes read + write per launch)",
                 "peak_source": f"{peak_kind} hbm_gbs (copy bandwidth)", "algorithmic_bytes": int(alg[dom_name]),
                 "stage_ms": {n: round(s, 4) for n, s in zip(stage_names, stages)},
                 "substep_algorithmic_bytes": int(sub_bytes),
@@ -309,14 +321,11 @@ def run_ours(args, rank, world, local_rank, dist):
         sim.step(1)
         for i in range(len(scenes)):
             sim.positions(i, out=pinned[i])
-    e2e_t = time.perf_counter() - t0
-    e2e_t_t = torch.tensor([e2e_t], dtype=torch.float64, device=f"cuda:{local_rank}")
-    if dist is not None:
-        dist.all_reduce(e2e_t_t, op=dist.ReduceOp.MAX)
+    e2e_t = reduce_max(dist, time.perf_counter() - t0, device=f"cuda:{local_rank}")
     sur = None
     if world == 1 and not args.no_surrogate:
         sur = surrogate_leg(args, sim, scenes, stream, flush, t_max_s * 1e3 / args.steps)
-    e2e = {"value": total_particles * e2e_steps / float(e2e_t_t.item()), "unit": UNIT,
+    e2e = {"value": total_particles * e2e_steps / e2e_t, "unit": UNIT,
            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(n_part * d * 4),
            "how": "mpm_step(h, 1) then mpm_get_positions into page-locked host memory every substep, wall clock "
                   "(the reference's loop: step() copies positions to the host every substep); "
