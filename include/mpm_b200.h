@@ -184,6 +184,20 @@ int mpm_num_particles(mpm_handle *h, int scene, int64_t *n);
  * positions, in creation order, as float x[N*dim].  cap is in floats. */
 int mpm_get_positions(mpm_handle *h, int scene, float *host_out, size_t cap);
 
+/* Same as mpm_get_positions without blocking: the positions after every
+ * substep enqueued so far are gathered on the handle's stream and copied to
+ * host_out on a second stream, so that substeps enqueued next run while the
+ * copy crosses to the host (the reference copies positions to host memory
+ * synchronously in every step(), MPMCUDA.cu:905-909, and reads them each
+ * loop iteration, main.cpp:206-210).  host_out should be
+ * page-locked for the copy to overlap, and must not be read or freed before
+ * mpm_wait_positions(h, *ticket) (or mpm_synchronize) returns.  Up to three
+ * copies can be in flight; a fourth waits, on the device, for the oldest.
+ * scene < 0 copies every scene's positions, concatenated in scene order. */
+int mpm_get_positions_async(mpm_handle *h, int scene, float *host_out, size_t cap,
+                            int64_t *ticket);
+int mpm_wait_positions(mpm_handle *h, int64_t ticket);
+
 /* Full particle state of one scene in creation order (the reference's device
  * arrays, MPMSimulator.cuh:37-43).  Any pointer may be NULL to skip it. */
 int mpm_get_state(mpm_handle *h, int scene, float *x, float *v, float *C, float *F,

@@ -72,6 +72,8 @@ EXPORTS = {
     "mpm_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "mpm_num_particles": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]),
     "mpm_get_positions": (C.c_int, [C.c_void_p, C.c_int, _FP, C.c_size_t]),
+    "mpm_get_positions_async": (C.c_int, [C.c_void_p, C.c_int, _FP, C.c_size_t, C.POINTER(C.c_int64)]),
+    "mpm_wait_positions": (C.c_int, [C.c_void_p, C.c_int64]),
     "mpm_get_state": (C.c_int, [C.c_void_p, C.c_int, _FP, _FP, _FP, _FP, _FP]),
     "mpm_set_state": (C.c_int, [C.c_void_p, C.c_int, _FP, _FP, _FP, _FP, _FP]),
     "mpm_get_grid": (C.c_int, [C.c_void_p, C.c_int, _FP, _FP]),

@@ -142,6 +142,24 @@ int mpm_get_positions(mpm_handle* h, int scene, float* x, size_t cap) {
     return h->eng.get_positions(scene, x);
 }
 
+int mpm_get_positions_async(mpm_handle* h, int scene, float* x, size_t cap, int64_t* ticket) {
+    if (!h || !x) return fail(h, MPM_ERR_INVALID, "mpm_get_positions_async: bad argument");
+    if (scene >= (int)h->eng.scenes_h.size())
+        return fail(h, MPM_ERR_INVALID, "mpm_get_positions_async: scene %d out of range", scene);
+    size_t need = (size_t)(scene < 0 ? h->eng.n_particles : h->eng.scene_count[scene]) * h->eng.dim;
+    if (cap < need)
+        return fail(h, MPM_ERR_INVALID, "mpm_get_positions_async: cap %zu < %zu floats", cap, need);
+    long long t = -1;
+    const int rc = h->eng.get_positions_async(scene, x, &t);
+    if (ticket) *ticket = t;
+    return rc;
+}
+
+int mpm_wait_positions(mpm_handle* h, int64_t ticket) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_wait_positions: NULL handle");
+    return h->eng.wait_positions(ticket);
+}
+
 int mpm_get_state(mpm_handle* h, int scene, float* x, float* v, float* C, float* F, float* aux) {
     if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_get_state: NULL handle");
     if (scene < 0 || scene >= (int)h->eng.scenes_h.size())

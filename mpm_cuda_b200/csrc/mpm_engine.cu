@@ -538,6 +538,15 @@ void Engine::release() {
     chunks = nullptr;
     scan_tmp = nullptr;
     pos_out = nullptr;
+    if (copy_stream) cudaStreamSynchronize(copy_stream);
+    for (auto& sl : pos_slots) {
+        cudaFree(sl.dev);
+        if (sl.gathered) cudaEventDestroy(sl.gathered);
+        if (sl.copied) cudaEventDestroy(sl.copied);
+        sl = PosSlot{};
+    }
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    copy_stream = nullptr;
     sur_counts = nullptr;
     sur = nullptr;
     if (stream) cudaStreamDestroy(stream);
@@ -915,6 +924,7 @@ int Engine::clear_errors() {
 
 int Engine::sync_and_check() {
     MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
+    if (copy_stream) MPM_CUDA_TRY(cudaStreamSynchronize(copy_stream), "copy stream sync");
     uint32_t bits = 0;
     int rc = read_errors(&bits);
     if (rc != MPM_OK) return rc;
@@ -946,6 +956,57 @@ int Engine::get_positions(int scene, float* out) {
     MPM_CUDA_TRY(cudaMemcpyAsync(out, pos_out, (size_t)n * dim * sizeof(float), cudaMemcpyDeviceToHost, stream),
                  "positions download");
     MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
+    return MPM_OK;
+}
+
+// Positions of one scene (creation order) copied to the host without
+// blocking: the gather runs on the handle's stream after the substeps enqueued
+// so far, the copy on a second stream, so later substeps overlap the copy.
+// A ring of kPosSlots staging buffers; a slot is reused only after its
+// previous copy finished (a device-side wait of the handle's stream).
+int Engine::get_positions_async(int scene, float* out, long long* ticket) {
+    MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    if (!copy_stream) {  // first use: the stream is created last, so a failed set-up is retried
+        for (auto& sl : pos_slots) {
+            if (!sl.dev)
+                MPM_CUDA_TRY(cudaMalloc((void**)&sl.dev, (size_t)std::max<long long>(cap, 1) * dim * sizeof(float)),
+                             "position staging");
+            if (!sl.gathered) MPM_CUDA_TRY(cudaEventCreateWithFlags(&sl.gathered, cudaEventDisableTiming), "event");
+            if (!sl.copied) MPM_CUDA_TRY(cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming), "event");
+        }
+        MPM_CUDA_TRY(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking), "copy stream");
+    }
+    const long long t = next_ticket++;
+    PosSlot& sl = pos_slots[t % kPosSlots];
+    if (sl.ticket >= 0) MPM_CUDA_TRY(cudaStreamWaitEvent(stream, sl.copied, 0), "slot reuse wait");
+    sl.ticket = t;
+    // scene < 0: every scene, concatenated in creation order
+    const long long b = scene < 0 ? 0 : scene_begin[scene], n = scene < 0 ? n_particles : scene_count[scene];
+    if (n > 0) {
+        k_gather_positions<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(st[cur], ids[cur], n_particles, cap, dim,
+                                                                              b, b + n, sl.dev);
+        MPM_CUDA_TRY(cudaGetLastError(), "gather launch");
+    }
+    MPM_CUDA_TRY(cudaEventRecord(sl.gathered, stream), "event record");
+    MPM_CUDA_TRY(cudaStreamWaitEvent(copy_stream, sl.gathered, 0), "copy wait");
+    if (n > 0)
+        MPM_CUDA_TRY(cudaMemcpyAsync(out, sl.dev, (size_t)n * dim * sizeof(float), cudaMemcpyDeviceToHost, copy_stream),
+                     "positions download");
+    MPM_CUDA_TRY(cudaEventRecord(sl.copied, copy_stream), "event record");
+    if (ticket) *ticket = t;
+    return MPM_OK;
+}
+
+// Waits until the copy of `ticket` has reached the host.  A slot reused by a
+// later ticket is waited for through that later copy, which the handle's
+// stream started only after the earlier one had finished.
+int Engine::wait_positions(long long ticket) {
+    if (ticket < 0 || ticket >= next_ticket) {
+        last_error = "mpm_wait_positions: unknown ticket";
+        return MPM_ERR_INVALID;
+    }
+    MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    MPM_CUDA_TRY(cudaEventSynchronize(pos_slots[ticket % kPosSlots].copied), "positions wait");
     return MPM_OK;
 }
 

@@ -68,6 +68,18 @@ struct Engine {
     int* active = nullptr;
     int* blk_epoch = nullptr;
     float* pos_out = nullptr;  // gathered positions (creation order)
+    // asynchronous position reads: a ring of staging buffers, each gathered on
+    // `stream` and copied to the host on `copy_stream`; created on first use
+    static constexpr int kPosSlots = 3;
+    struct PosSlot {
+        float* dev = nullptr;
+        cudaEvent_t gathered = nullptr;  // gather done (recorded on stream)
+        cudaEvent_t copied = nullptr;    // host copy done (recorded on copy_stream)
+        long long ticket = -1;           // last ticket that used the slot
+    };
+    PosSlot pos_slots[kPosSlots];
+    cudaStream_t copy_stream = nullptr;
+    long long next_ticket = 0;
     int fused_ctas[3] = {0, 0, 0};  // persistent CTAs per material kernel
     int cfg = 1;                     // index into kFusedCfgs
     // learned stress (MPM_STRESS_SURROGATE): the network, the version of its
@@ -105,6 +117,8 @@ struct Engine {
     int stress_stats(int64_t* net, int64_t* fallback);
     int profile_stages(int n, float* out_ms, int n_out, int* n_written);
     int get_positions(int scene, float* out);
+    int get_positions_async(int scene, float* out, long long* ticket);
+    int wait_positions(long long ticket);
     int bin_stats(int64_t* fallbacks, int64_t* rebins);
     void set_config(int ci);
     int autotune(int steps, float* best_ms);

@@ -237,6 +237,19 @@ class Simulation:
         self._check(self._lib.mpm_get_positions(self._h, scene, L.fptr(out), out.size))
         return out
 
+    def positions_async(self, out: np.ndarray, scene: int = 0) -> int:
+        """Starts copying the positions after the substeps enqueued so far into
+        `out` (float32 (n, dim), page-locked for overlap) and returns a ticket;
+        `out` is valid after wait_positions(ticket)."""
+        n = self.num_particles(scene)  # scene < 0: every scene
+        assert out.dtype == np.float32 and out.flags["C_CONTIGUOUS"] and out.size >= n * self.dim
+        t = C.c_int64()
+        self._check(self._lib.mpm_get_positions_async(self._h, scene, L.fptr(out), out.size, C.byref(t)))
+        return t.value
+
+    def wait_positions(self, ticket: int):
+        self._check(self._lib.mpm_wait_positions(self._h, ticket))
+
     def get_state(self, scene: int = 0) -> dict:
         n, d = self.num_particles(scene), self.dim
         st = {"x": np.empty((n, d), np.float32), "v": np.empty((n, d), np.float32),

@@ -335,3 +335,39 @@ def test_deterministic_after_binned_steps_is_reproducible(gpu):
             outs.append(sim.get_state(0))
     for k in ("x", "v", "C", "F", "aux"):
         assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+def test_async_positions_match_synchronous_reads(gpu):
+    # deterministic P2G: two handles stepping the same state agree bitwise, so
+    # the pipelined reads (substep k+1 enqueued before step k's copy is waited
+    # for, more copies in flight than staging slots) must equal blocking reads
+    sc = blob_scene(3, "jello", seed=90)
+    n_steps = 6
+    with Simulation([sc], p2g_mode=L.P2G_DETERMINISTIC) as ref, \
+            Simulation([sc], p2g_mode=L.P2G_DETERMINISTIC) as sim:
+        want = []
+        for _ in range(n_steps):
+            ref.step(1)
+            want.append(ref.positions(0).copy())
+        n = sim.num_particles(0)
+        outs = [np.empty((n, 3), np.float32) for _ in range(n_steps)]
+        tickets = []
+        for k in range(n_steps):
+            sim.step_async(1)
+            tickets.append(sim.positions_async(outs[k], scene=0))
+        for k in reversed(range(n_steps)):
+            sim.wait_positions(tickets[k])
+            assert np.array_equal(outs[k], want[k]), k
+        with pytest.raises(L.MPMError) as e:
+            sim.wait_positions(tickets[-1] + 1)
+        assert e.value.code == L.ERR_INVALID
+
+
+def test_async_positions_of_all_scenes(gpu):
+    scenes = [blob_scene(3, "jello", seed=91), blob_scene(3, "snow", seed=92)]
+    with Simulation(scenes) as sim:
+        sim.step(2)
+        sync = np.concatenate([sim.positions(0), sim.positions(1)])
+        out = np.empty_like(sync)
+        sim.wait_positions(sim.positions_async(out, scene=-1))
+        assert np.array_equal(out, sync)
