@@ -151,7 +151,8 @@ void mpm_default_options(mpm_options *opt);
 
 /* Replaces MPMSimulator::MPMSimulator(gap, dt, nx, ny, nz, ppc, objs)
  * (src/simulator/MPMSimulator.cuh:92-96, MPMSimulator.cpp:178-285): builds
- * n_scenes independent scenes on one device.  opt may be NULL. */
+ * n_scenes independent scenes on one device.  opt may be NULL.  A scene's
+ * grid (rounded up to whole blocks) holds fewer than 2^31 nodes. */
 int mpm_create(const mpm_scene_desc *scenes, int n_scenes, const mpm_options *opt,
                mpm_handle **out);
 

@@ -187,6 +187,10 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
         sp.block_off = block_off;
         sp.node_off = block_off * 64;
         sp.n_nodes = sp.n_blocks * 64;
+        if (sp.n_nodes > 0x7fffffffLL) {  // per-scene node offsets are 32-bit in the kernels
+            std::snprintf(buf, sizeof(buf), "mpm_create: scene %d has more than 2^31 grid nodes", s);
+            return bad(MPM_ERR_INVALID, buf);
+        }
         block_off += sp.n_blocks;
         scenes_h[s] = sp;
         scene_begin[s] = p_off;

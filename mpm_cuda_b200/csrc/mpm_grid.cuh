@@ -27,6 +27,34 @@ __device__ __forceinline__ long long node_index(const SceneParams& sc, int ix, i
     return sc.node_off + blk * 64 + in;
 }
 
+// Node indices of a 3^D stencil, relative to the scene's first node.  The
+// blocked index is separable per axis, so index(ox, oy, oz) = x[ox] + y[oy] +
+// z[oz] (equal to node_index - node_off): 9 offsets computed once instead of
+// the block/local split of 27 nodes.  A scene has fewer than 2^31 nodes
+// (checked at creation), so the offsets are 32-bit.
+template <int D>
+struct StencilIndex {
+    int x[3], y[3], z[3];
+    __device__ __forceinline__ StencilIndex(const SceneParams& sc, const int* base) {
+        constexpr int S = BlockShape<D>::SHIFT;
+        constexpr int M = BlockShape<D>::SIDE - 1;
+        constexpr int SIDE = BlockShape<D>::SIDE;
+#pragma unroll
+        for (int o = 0; o < 3; ++o) {
+            const int ix = base[0] + o, iy = base[1] + o;
+            x[o] = (ix >> S) * 64 + (ix & M);
+            y[o] = (iy >> S) * sc.nb[0] * 64 + (iy & M) * SIDE;
+            if (D == 3) {
+                const int iz = base[2] + o;
+                z[o] = (iz >> S) * sc.nb[0] * sc.nb[1] * 64 + (iz & M) * SIDE * SIDE;
+            } else {
+                z[o] = 0;
+            }
+        }
+    }
+    __device__ __forceinline__ int operator()(int ox, int oy, int oz) const { return x[ox] + y[oy] + z[oz]; }
+};
+
 // scene owning global block `b` (binary search over block_off)
 __device__ __forceinline__ int scene_of_block(const SceneParams* scenes, int n_scenes, long long b) {
     int lo = 0, hi = n_scenes - 1;

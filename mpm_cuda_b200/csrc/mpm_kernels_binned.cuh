@@ -165,8 +165,10 @@ __device__ __forceinline__ long long block_of_node(const SceneParams& sc, int ix
 template <int D>
 __device__ __forceinline__ void p2g_global(const Stencil<D>& st, const P2GSource<D>& src, const SceneParams& sc,
                                            float4* grid_mom, unsigned* blk_flag, int* active, int* n_active) {
+    const StencilIndex<D> ix(sc, st.base);
+    float4* g = grid_mom + sc.node_off;
     p2g_scatter<D>(st, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 c) {
-        atomicAdd(&grid_mom[node_index<D>(sc, st.base[0] + ox, st.base[1] + oy, D == 3 ? st.base[2] + oz : 0)], c);
+        atomicAdd(&g[ix(ox, oy, D == 3 ? oz : 0)], c);
     });
     // the stencil spans at most 2 blocks per axis: mark its corner blocks
 #pragma unroll
@@ -323,9 +325,9 @@ __device__ __forceinline__ void g2p_window(const Stencil<D>& st, const int* o, c
         }, acc);
     } else {
         atomicAdd(A.fallback, 1u);
-        g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) {
-            return A.grid_vel[node_index<D>(sc, st.base[0] + ox, st.base[1] + oy, D == 3 ? st.base[2] + oz : 0)];
-        }, acc);
+        const StencilIndex<D> ix(sc, st.base);
+        const float4* g = A.grid_vel + sc.node_off;
+        g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) { return g[ix(ox, oy, D == 3 ? oz : 0)]; }, acc);
     }
 }
 
@@ -397,9 +399,10 @@ template <int D>
 __device__ __forceinline__ void scatter_global(const Stencil<D>& sn, const P2GSource<D>& src, const SceneParams& sc,
                                                const int* o, const FusedArgs& A, unsigned* touched) {
     if (in_window<D>(sn.base, o)) {
+        const StencilIndex<D> ix(sc, sn.base);
+        float4* g = A.grid_mom + sc.node_off;
         p2g_scatter<D>(sn, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 cc) {
-            atomicAdd(&A.grid_mom[node_index<D>(sc, sn.base[0] + ox, sn.base[1] + oy, D == 3 ? sn.base[2] + oz : 0)],
-                      cc);
+            atomicAdd(&g[ix(ox, oy, D == 3 ? oz : 0)], cc);
         });
         atomicOr(touched, touched_bits<D>(sn.base[0] - o[0], sn.base[1] - o[1], D == 3 ? sn.base[2] - o[2] : 0));
     } else {

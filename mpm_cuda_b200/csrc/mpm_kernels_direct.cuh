@@ -48,8 +48,10 @@ __global__ void __launch_bounds__(128) k_p2g_direct(ParticleBuf pb, long long n,
     }
     P2GSource<D> src;
     particle_stress_source<D>(v, C, F, aux, g, sc, src);
+    const StencilIndex<D> ix(sc, st.base);
+    float4* gs = grid + sc.node_off;
     p2g_scatter<D>(st, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 c) {
-        atomicAdd(&grid[node_index<D>(sc, st.base[0] + ox, st.base[1] + oy, D == 3 ? st.base[2] + oz : 0)], c);
+        atomicAdd(&gs[ix(ox, oy, D == 3 ? oz : 0)], c);
     });
 }
 
@@ -100,9 +102,9 @@ __global__ void __launch_bounds__(128) k_g2p_direct(ParticleBuf pb, long long n,
     }
     G2PAcc<D> acc;
     const float inv_h = sc.inv_h;
-    g2p_gather<D>(st, inv_h, [&](int ox, int oy, int oz) {
-        return __ldg(&grid[node_index<D>(sc, st.base[0] + ox, st.base[1] + oy, D == 3 ? st.base[2] + oz : 0)]);
-    }, acc);
+    const StencilIndex<D> ix(sc, st.base);
+    const float4* gs = grid + sc.node_off;
+    g2p_gather<D>(st, inv_h, [&](int ox, int oy, int oz) { return __ldg(&gs[ix(ox, oy, D == 3 ? oz : 0)]); }, acc);
     float F[D * D], aux = s[P::AUX * cap + i];
     if (g.type != WATER) {
 #pragma unroll
