@@ -76,16 +76,31 @@ MPM_HD void inverse(const float* A, float* Ai) {
 //   3. one Newton-Schulz polish of V:  V <- V (3 I - V^T V) / 2
 //   4. sort by eigenvalue, B = F V, Gram-Schmidt QR of B -> U, s
 
+// x / y with the hardware's approximate division on the device (y a normal
+// magnitude here); exact division on the host
+MPM_HD float fast_div(float x, float y) {
+#ifdef __CUDA_ARCH__
+    return __fdividef(x, y);
+#else
+    return x / y;
+#endif
+}
+
 // one Jacobi rotation on the (p,q) pair of the symmetric S (stored as 3x3)
 template <int P, int Q>
 MPM_HD void jacobi_rotate(float* S, float* V) {
     constexpr int R = 3 - P - Q;  // the remaining index
     const float spq = S[P * 3 + Q];
     const float diff = S[Q * 3 + Q] - S[P * 3 + P];
-    const float root = sqrtf(fmaf(diff, diff, 4.f * spq * spq));
+    // tan of the rotation angle (0 when the pair is already diagonal).  The
+    // approximate square root and quotient only perturb the angle: c and s
+    // below form an exact rotation for any t, so orthogonality does not suffer
+    // (below 1e-30 the pair counts as diagonal: keeps both operations on
+    // normal numbers)
+    const float q = fmaf(diff, diff, 4.f * spq * spq);
+    const float root = q > 1e-30f ? q * rsqrtf(q) : 0.f;
     const float den = fabsf(diff) + root;
-    // tan of the rotation angle; 0 when the pair is already diagonal
-    float t = den > 0.f ? (2.f * spq) / den : 0.f;
+    float t = den > 1e-30f ? fast_div(2.f * spq, den) : 0.f;
     t = diff < 0.f ? -t : t;
     const float c = rsqrtf(fmaf(t, t, 1.f));
     const float s = t * c;
