@@ -306,8 +306,15 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     while (key_bits < 64 && (1LL << (key_bits - 12)) < total_blocks) ++key_bits;
     det_key_bits = 1;
     while (det_key_bits < 64 && (1LL << det_key_bits) <= total_blocks * 64) ++det_key_bits;
-    cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp_bytes, keys[0], keys[1], vals[0], vals[1], (int)cap, 0,
-                                    key_bits);
+    // binning keys are sorted as 32-bit words when they fit (fewer bytes per
+    // radix pass); the key buffers are allocated as 64-bit either way
+    if (key_bits <= 32) {
+        cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp_bytes, keys32(0), keys32(1), vals[0], vals[1], (int)cap, 0,
+                                        key_bits);
+    } else {
+        cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp_bytes, keys[0], keys[1], vals[0], vals[1], (int)cap, 0,
+                                        key_bits);
+    }
     {
         size_t det_bytes = 0;
         cub::DeviceRadixSort::SortPairs(nullptr, det_bytes, keys[0], keys[1], vals[0], vals[1], (int)cap, 0, 64);
@@ -600,15 +607,28 @@ void Engine::enqueue_rebin(int from) {
     const long long n_segs = total_blocks * 4;
     cudaMemsetAsync(counters + CNT_CHUNKS, 0, kMats * sizeof(int), stream);
     if (n_particles > 0) {
-        if (dim == 3)
-            k_bin_key<3><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d,
-                                                                            keys[0], vals[0], cell_count, seg_count);
-        else
-            k_bin_key<2><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d,
-                                                                            keys[0], vals[0], cell_count, seg_count);
-        note_launch("k_bin_key");
-        cub::DeviceRadixSort::SortPairs(sort_tmp, sort_tmp_bytes, keys[0], keys[1], vals[0], vals[1],
-                                        (int)n_particles, 0, key_bits, stream);
+        const unsigned nb = grid_blocks(n_particles, 256);
+        if (key_bits <= 32) {
+            if (dim == 3)
+                k_bin_key<3, unsigned><<<nb, 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d, keys32(0),
+                                                               vals[0], cell_count, seg_count);
+            else
+                k_bin_key<2, unsigned><<<nb, 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d, keys32(0),
+                                                               vals[0], cell_count, seg_count);
+            note_launch("k_bin_key");
+            cub::DeviceRadixSort::SortPairs(sort_tmp, sort_tmp_bytes, keys32(0), keys32(1), vals[0], vals[1],
+                                            (int)n_particles, 0, key_bits, stream);
+        } else {
+            if (dim == 3)
+                k_bin_key<3, unsigned long long><<<nb, 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d,
+                                                                         keys[0], vals[0], cell_count, seg_count);
+            else
+                k_bin_key<2, unsigned long long><<<nb, 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d,
+                                                                         keys[0], vals[0], cell_count, seg_count);
+            note_launch("k_bin_key");
+            cub::DeviceRadixSort::SortPairs(sort_tmp, sort_tmp_bytes, keys[0], keys[1], vals[0], vals[1],
+                                            (int)n_particles, 0, key_bits, stream);
+        }
         note_launch("cub::DeviceRadixSort::SortPairs");
         if (dim == 3)
             k_bin_gather<3><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), buf(to), n_particles,
@@ -624,7 +644,14 @@ void Engine::enqueue_rebin(int from) {
                                                                 counters + CNT_CHUNKS, kFusedCfgs[cfg].chunk);
     note_launch("k_make_chunks");
     if (n_particles > 0)
-        k_bin_reset<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys[1], n_particles, cell_count, seg_count);
+    {
+        if (key_bits <= 32)
+            k_bin_reset<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys32(1), n_particles, cell_count,
+                                                                           seg_count);
+        else
+            k_bin_reset<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys[1], n_particles, cell_count,
+                                                                           seg_count);
+    }
     note_launch("k_bin_reset");
     k_count_rebin<<<1, 1, 0, stream>>>(counters + CNT_REBINS);
     note_launch("k_count_rebin");

@@ -47,6 +47,8 @@ struct Engine {
 
     // binning and block activity
     unsigned long long* keys[2] = {nullptr, nullptr};  // radix sort keys in / out
+    // the same buffers as 32-bit keys (binning keys of at most 32 bits)
+    unsigned* keys32(int p) const { return reinterpret_cast<unsigned*>(keys[p]); }
     unsigned* vals[2] = {nullptr, nullptr};            // particle index in / sorted
     int* cell_count = nullptr;  // per node of every block: particles whose base is that node
     int* cell_end = nullptr;    // deterministic mode: end of each base node's records

@@ -77,11 +77,11 @@ __device__ __forceinline__ void home_of(const SceneParams& sc, const float* x, l
 }
 
 // sort key (block, material, rank in cell, cell) and the identity payload
-template <int D>
+template <int D, class K>
 __global__ void __launch_bounds__(256) k_bin_key(ParticleBuf pb, long long n, const GroupParams* __restrict__ groups,
-                                                 const SceneParams* __restrict__ scenes,
-                                                 unsigned long long* __restrict__ keys, unsigned* __restrict__ vals,
-                                                 int* __restrict__ cell_count, int* __restrict__ seg_count) {
+                                                 const SceneParams* __restrict__ scenes, K* __restrict__ keys,
+                                                 unsigned* __restrict__ vals, int* __restrict__ cell_count,
+                                                 int* __restrict__ seg_count) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float x[D];
@@ -94,8 +94,9 @@ __global__ void __launch_bounds__(256) k_bin_key(ParticleBuf pb, long long n, co
     home_of<D>(sc, x, b, c);
     const int r = min(atomicAdd(&cell_count[b * 64 + c], 1), kMaxRank);
     atomicAdd(&seg_count[b * 4 + g.type], 1);
-    keys[i] = ((unsigned long long)b << 12) | ((unsigned long long)g.type << 10) | ((unsigned long long)r << 6) |
-              (unsigned long long)c;
+    // K is 32-bit when the block index fits in 20 bits
+    keys[i] = (K)(((unsigned long long)b << 12) | ((unsigned long long)g.type << 10) | ((unsigned long long)r << 6) |
+                  (unsigned long long)c);
     vals[i] = (unsigned)i;
 }
 
@@ -136,7 +137,8 @@ static __global__ void __launch_bounds__(256) k_make_chunks(const int* __restric
 }
 
 // zero the cell and segment counters the last k_bin_key touched
-static __global__ void __launch_bounds__(256) k_bin_reset(const unsigned long long* __restrict__ keys, long long n,
+template <class K>
+__global__ void __launch_bounds__(256) k_bin_reset(const K* __restrict__ keys, long long n,
                                                    int* __restrict__ cell_count, int* __restrict__ seg_count) {
     const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
