@@ -338,7 +338,8 @@ __device__ __forceinline__ void g2p_window(const Stencil<D>& st, const int* o, c
 template <int D, int MAT>
 __device__ __forceinline__ unsigned update_and_store(const G2PAcc<D>& acc, const SceneParams& sc, const GroupParams& g,
                                                      float* __restrict__ S, long long cap, long long i, float* x,
-                                                     float* v, float* Cn, float* F, float& aux) {
+                                                     float* v, float* Cn, float* F, float& aux,
+                                                     ElasticSVD<D>* keep = nullptr) {
     using P = Planes<D>;
     aux = 1.f;
     if (MAT != JELLO) aux = S[P::AUX * cap + i];
@@ -349,7 +350,7 @@ __device__ __forceinline__ unsigned update_and_store(const G2PAcc<D>& acc, const
 #pragma unroll
         for (int k = 0; k < D * D; ++k) F[k] = (k % (D + 1) == 0) ? 1.f : 0.f;
     }
-    const unsigned err = material_update<D, MAT>(acc, sc.dt, g, F, aux);
+    const unsigned err = material_update<D, MAT>(acc, sc.dt, g, F, aux, keep);
     const float c4 = 4.f * sc.inv_h;
 #pragma unroll
     for (int a = 0; a < D; ++a) {
@@ -506,13 +507,15 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
             // loaded after the gather, its register peak
             const GroupParams g = A.groups[pb.grp[i]];
             float F[D * D], Cn[D * D], v[D], aux;
-            err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux);
+            ElasticSVD<D> esvd;  // snow: the plasticity step's decomposition, reused by the stress
+            err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux, MAT == SNOW ? &esvd : nullptr);
 
             // ---- stress + P2G of the next substep
             Stencil<D> sn;
             if (make_stencil<D>(x, sc, sn, err)) {
                 P2GSource<D> src;
-                particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc, src);
+                if (MAT == SNOW) snow_stress_source<D>(v, Cn, esvd, aux, g, sc, src);
+                else particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc, src);
                 scatter_global<D>(sn, src, sc, o, A, tb);
             }
         }

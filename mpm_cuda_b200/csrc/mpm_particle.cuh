@@ -116,6 +116,48 @@ __device__ __forceinline__ void particle_stress_source(const float* v, const flo
     src.m = g.p_mass;
 }
 
+// Left singular vectors and clamped singular values of snow's new elastic F
+// (Fe = U diag(s) V^T), kept by material_update for the stress of the next
+// P2G: tau(Fe) = U diag(2 mu s (s - 1)) U^T + lambda J (J - 1) I, J = prod s,
+// needs no second decomposition.
+template <int D>
+struct ElasticSVD {
+    float U[D * D];
+    float s[D];
+};
+
+// Snow's source from the decomposition its plasticity step kept (equal to
+// particle_stress_source of Fe = U diag(s) V^T): hardening exp(xi (1 - Jp))
+// (MPMCUDA.cu:342-347) and the fixed-corotated stress of U, s.
+template <int D>
+__device__ __forceinline__ void snow_stress_source(const float* v, const float* C, const ElasticSVD<D>& e,
+                                                   float aux, const GroupParams& g, const SceneParams& sc,
+                                                   P2GSource<D>& src) {
+    const float hc = expf(g.xi * (1.f - aux));
+    const float mu = g.mu * hc, la = g.lambda * hc;
+    float J = 1.f, dg[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        J *= e.s[k];
+        dg[k] = 2.f * mu * e.s[k] * (e.s[k] - 1.f);
+    }
+    const float iso = la * J * (J - 1.f);
+    const float kf = -sc.dt * g.p_vol;
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+            float acc = (i == j) ? iso : 0.f;
+#pragma unroll
+            for (int k = 0; k < D; ++k) acc = fmaf(e.U[i * D + k] * dg[k], e.U[j * D + k], acc);
+            src.A[i * D + j] = kf * acc;
+            src.mC[i * D + j] = g.p_mass * C[i * D + j];
+        }
+#pragma unroll
+    for (int a = 0; a < D; ++a) src.mv[a] = g.p_mass * v[a];
+    src.m = g.p_mass;
+}
+
 // the same source from a given Kirchhoff stress (the surrogate path)
 template <int D>
 __device__ __forceinline__ void source_from_tau(const float* v, const float* C, const float* tau, const GroupParams& g,
@@ -403,7 +445,8 @@ __device__ __forceinline__ void p2g_scatter(const Stencil<D>& st, const P2GSourc
 // MPMWater.py:138).  Updates F / aux in place, returns error bits.
 template <int D, int MAT = -1>
 __device__ __forceinline__ unsigned material_update(const G2PAcc<D>& acc, float dt,
-                                                    const GroupParams& g, float* F, float& aux) {
+                                                    const GroupParams& g, float* F, float& aux,
+                                                    ElasticSVD<D>* keep = nullptr) {
     unsigned err = 0;
     if (is_mat<MAT>(g, WATER)) {
         float div = 0.f;
@@ -441,6 +484,12 @@ __device__ __forceinline__ unsigned material_update(const G2PAcc<D>& acc, float 
                 for (int k = 0; k < D; ++k) acc2 = fmaf(U[i * D + k] * s[k], V[j * D + k], acc2);
                 F[i * D + j] = acc2;
             }
+        if (keep) {
+#pragma unroll
+            for (int k = 0; k < D * D; ++k) keep->U[k] = U[k];
+#pragma unroll
+            for (int k = 0; k < D; ++k) keep->s[k] = s[k];
+        }
         // det Fp_new = det(Fe_new^-1 Fe_trial Fp) = det_trial / det_new * det Fp
         aux = aux * (det_trial / det_new);
         if (!(aux > 0.f)) err |= ERR_DET;
