@@ -286,8 +286,9 @@ int mpm_step_noalloc(const mpm_scene_desc *scene, float *state, int64_t plane_st
  * Learned stress surrogate.  No counterpart in the reference, whose stress
  * pass always takes an SVD (MPMCUDA.cu:87-134, 229-264).  A BF16 MLP
  * 10 -> 64 -> 64 -> 9 (SiLU) predicts the residual of sqrt(F F^T) beyond its
- * second-order series; the Kirchhoff stress of jello and of snow's elastic
- * part follows from it without an SVD.  Training and inference run on the
+ * second-order series; the Kirchhoff stress of jello follows from it without
+ * an SVD (snow's stress already reuses the decomposition of its plasticity
+ * clamp and keeps the plain path).  Training and inference run on the
  * GPU's tensor cores; particles outside the training envelope, or whose error
  * estimate is above skew_tol, take the SVD path.
  * ---------------------------------------------------------------------- */
@@ -342,10 +343,10 @@ int mpm_surrogate_set_params(mpm_surrogate *s, const float *params, const float 
 int mpm_surrogate_save(mpm_surrogate *s, const char *path);
 int mpm_surrogate_load(const char *path, int device, mpm_surrogate **out);
 
-/* Selects the stress of the 3D jello and snow groups: MPM_STRESS_PLAIN, or
+/* Selects the stress of the 3D jello groups: MPM_STRESS_PLAIN, or
  * MPM_STRESS_SURROGATE with network s (kept alive by the caller while the
  * handle uses it; call again after retraining s).  Needs MPM_P2G_ATOMIC;
- * water and 2D scenes keep the plain stress. */
+ * snow, water and 2D scenes keep the plain stress. */
 int mpm_set_stress_mode(mpm_handle *h, int mode, mpm_surrogate *s);
 
 /* Particles whose stress came from the network / from the SVD fallback in

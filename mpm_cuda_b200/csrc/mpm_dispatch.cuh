@@ -13,7 +13,7 @@ using SurFn = void (*)(ParticleBuf, FusedArgs, SurArgs);
 
 // k_g2p2g<dim, mat, kFusedCfgs[ci]>
 FusedFn fused_fn(int dim, int mat, int ci);
-// k_g2p2g_sur<mat, kFusedCfgs[ci]> (3D jello and snow)
-SurFn sur_fn(int mat, int ci);
+// k_g2p2g_sur<kFusedCfgs[ci]> (3D jello)
+SurFn sur_fn(int ci);
 
 }  // namespace mpm

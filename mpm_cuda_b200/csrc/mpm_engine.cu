@@ -400,10 +400,10 @@ void Engine::sur_occupancy() {
         int per_sm = 0;
         // the network rows live in dynamic shared memory; with the windows and
         // weights they can exceed the 48 KB a kernel gets without opting in
-        if (cudaFuncSetAttribute(sur_fn(mat, cfg), cudaFuncAttributeMaxDynamicSharedMemorySize, sur_dyn_smem(ch)) !=
+        if (cudaFuncSetAttribute(sur_fn(cfg), cudaFuncAttributeMaxDynamicSharedMemorySize, sur_dyn_smem(ch)) !=
             cudaSuccess)
             cudaGetLastError();  // not fatal here: the occupancy query and the launch report it
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sur_fn(mat, cfg), ch, sur_dyn_smem(ch)) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sur_fn(cfg), ch, sur_dyn_smem(ch)) !=
             cudaSuccess) {
             cudaGetLastError();
             per_sm = 1;
@@ -703,7 +703,7 @@ void Engine::enqueue_g2p2g(int parity) {
         if (sur_kernel(mat)) {
             const SurArgs SA{&sur->weights->f, sur->meta, sur_counts};
             const int ch = kFusedCfgs[cfg].chunk;
-            sur_fn(mat, cfg)<<<sur_ctas[mat], ch, sur_dyn_smem(ch), stream>>>(buf(parity), A, SA);
+            sur_fn(cfg)<<<sur_ctas[mat], ch, sur_dyn_smem(ch), stream>>>(buf(parity), A, SA);
             note_launch("k_g2p2g_sur");
         } else {
             fused_fn(dim, mat, cfg)<<<fused_ctas[mat], kFusedCfgs[cfg].chunk, 0, stream>>>(buf(parity), A);
@@ -1194,8 +1194,9 @@ int Engine::set_stress_mode(int mode, Surrogate* s) {
     MPM_CUDA_TRY(cudaMemset(sur_counts, 0, 2 * sizeof(unsigned long long)), "clear counters");
     sur = mode == MPM_STRESS_SURROGATE ? s : nullptr;
     opt.stress_mode = mode;
-    // eligible groups: 3D jello and snow
-    for (auto& g : groups_h) g.surrogate = (sur && dim == 3 && (g.type == JELLO || g.type == SNOW)) ? 1 : 0;
+    // eligible groups: 3D jello (snow's exact stress reuses its plasticity
+    // decomposition, so the network could only cost time there)
+    for (auto& g : groups_h) g.surrogate = (sur && dim == 3 && g.type == JELLO) ? 1 : 0;
     MPM_CUDA_TRY(cudaMemcpy(groups_d, groups_h.data(), groups_h.size() * sizeof(GroupParams), cudaMemcpyHostToDevice),
                  "group upload");
     sur_version = sur ? sur->version : -1;

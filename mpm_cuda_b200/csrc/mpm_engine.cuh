@@ -144,7 +144,8 @@ struct Engine {
     bool fused() const { return opt.p2g_mode == MPM_P2G_ATOMIC; }
     bool deterministic() const { return opt.p2g_mode == MPM_P2G_DETERMINISTIC; }
     bool direct() const { return opt.p2g_mode == MPM_P2G_DIRECT; }
-    bool sur_kernel(int mat) const { return sur && dim == 3 && (mat == JELLO || mat == SNOW); }
+    // jello only: snow's exact stress reuses its plasticity decomposition
+    bool sur_kernel(int mat) const { return sur && dim == 3 && mat == JELLO; }
     void sur_occupancy();
     int sur_refresh();
     void enqueue_det_p2g();

@@ -1,5 +1,6 @@
-// Fused substep with the learned stress (MPM_STRESS_SURROGATE), 3D jello and
-// snow.  Same pass as k_g2p2g (G2P, particle update, stress, P2G of the next
+// Fused substep with the learned stress (MPM_STRESS_SURROGATE), 3D jello.
+// (Snow's exact stress costs no decomposition of its own: it reuses the one of
+// its plasticity clamp, so snow keeps the plain kernel.)  Same pass as k_g2p2g (G2P, particle update, stress, P2G of the next
 // substep) with the stress of eligible particles taken from the BF16 MLP
 // (mpm_mlp.cuh) instead of the SVD in kirchhoff_fcr (MPMCUDA.cu:229-264):
 //   1. every thread: G2P, update, store the new state, write its network
@@ -29,13 +30,13 @@ struct SurArgs {
     unsigned long long* counts;  // [0] stresses from the network, [1] SVD fallbacks
 };
 
-template <int MAT, int CHUNK, int MINB>
+template <int CHUNK, int MINB>
 __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, FusedArgs A, SurArgs SA) {
     constexpr int D = 3;
+    constexpr int MAT = JELLO;
     using P = Planes<D>;
     using TS = TileShape<D>;
     static_assert(CHUNK % 32 == 0, "whole warps");
-    static_assert(MAT == JELLO || MAT == SNOW, "elastic materials only");
     constexpr int XS = kSurRowStride;
     __shared__ __align__(16) float4 tv[2][TS::VN];  // grid velocity windows (double-buffered)
     __shared__ __align__(16) mlp::Forward W;        // network weights
@@ -103,22 +104,15 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
                 Cn[k] = __ldcg(S + (P::C + k) * cap + i);
                 F[k] = __ldcg(S + (P::F + k) * cap + i);
             }
-            if (MAT == SNOW) aux = __ldcg(S + P::AUX * cap + i);
             const GroupParams g = A.groups[gi];
             Stencil<D> sn;
             make_stencil<D>(x, sc, sn, err);  // the stencil found above
             float tau[D * D];
             bool use = false;
             if (eligible) {
-                float mu = g.mu, la = g.lambda;
-                if (MAT == SNOW) {
-                    // hardening exp(xi (1 - Jp)) (MPMCUDA.cu:342-347)
-                    const float hc = expf(g.xi * (1.f - aux));
-                    mu *= hc;
-                    la *= hc;
-                }
                 const float J = det<3>(F);
-                use = mlp::in_envelope(F, J, SA.meta) && mlp::tau_from_prediction(row, F, J, mu, la, SA.meta, tau);
+                use = mlp::in_envelope(F, J, SA.meta) &&
+                      mlp::tau_from_prediction(row, F, J, g.mu, g.lambda, SA.meta, tau);
             }
             P2GSource<D> src;
             if (use) {
