@@ -119,7 +119,7 @@ def build_workload(name: str, rank: int, world: int):
     if name == "c4":
         return shard(S.c4_batched(), rank, world), "c4 64 batched scenes (jello/snow/water)"
     if name == "c0":
-        return [S.c0_jello2d(seed=seed)], "c0 2D jello 128^2, 9000 particles"
+        return [S.c0_jello2d(seed=seed)], "c0 2D jello 128^2, 9000 particles, E=1e3 (MPMJello.py:12; E=1e4 breaks the CFL bound)"
     if name == "c2":
         return [S.c2_snow3d(seed=seed)], "c2 3D snow 256^3, two spheres r=0.12, 8 ppc"
     if name == "c3":

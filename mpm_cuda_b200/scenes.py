@@ -62,15 +62,20 @@ def make_group(mat: MaterialParams, x: np.ndarray, h: float, ppc: int, v0) -> Gr
 
 # ---------------------------------------------------------------- workloads
 
-def c0_jello2d(seed: int = 1234) -> Scene:
+def c0_jello2d(seed: int = 1234, E: float = 1e3) -> Scene:
     """2D jello as MPMJello.py: 128^2, dx = 1/128, N = 9000 uniform in a 0.2
-    square centred at (0.5, 0.6), v = (0, -1), E = 1e4, nu = 0.2, rho = 1,
+    square centred at (0.5, 0.6), v = (0, -1), nu = 0.2, rho = 1,
     p_vol = (dx/2)^2, dt = 1e-4, gravity -9.8, 3-cell wall as
-    MPMJello.py:92-95 (zero the wall-normal velocity moving into the wall)."""
+    MPMJello.py:92-95 (zero the wall-normal velocity moving into the wall).
+
+    E defaults to the script's 1e3 (MPMJello.py:12).  E = 1e4 with rho = 1
+    gives an elastic wave speed of 100 m/s and a CFL number
+    dt sqrt(E / rho) / dx = 1.28 > 1: the substep diverges (the FP64 oracle
+    within ~45 substeps)."""
     rng = np.random.default_rng(seed)
     n_grid, dx = 128, 1.0 / 128
     x = (rng.random((9000, 2)) * 0.2 + np.array([0.4, 0.5])).astype(np.float32)
-    mat = MaterialParams(L.JELLO, 1e4, 0.2, 1.0)
+    mat = MaterialParams(L.JELLO, E, 0.2, 1.0)
     vol = (dx * 0.5) ** 2
     g = Group(material=mat, p_mass=vol * 1.0, p_vol=vol, x=x, init_v=(0.0, -1.0))
     return Scene(dim=2, n=(n_grid, n_grid), h=dx, dt=1e-4, groups=[g], gravity=(0.0, -9.8),

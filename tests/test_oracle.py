@@ -210,3 +210,16 @@ def test_oracle_matches_reference_build_golden(path):
                 med = np.median(np.abs(got - ref)) / max(np.abs(ref).max(), 1e-30)
                 assert med < TOL_REF_MEDIAN[k], (f, k, med)
             off += m
+
+
+def test_c0_stated_stiffness_violates_the_cfl_bound():
+    """The 2D jello workload at E = 1e4 (rho = 1, dx = 1/128, dt = 1e-4) has an
+    elastic CFL number of 1.28 and diverges in the FP64 oracle; the script's
+    own E = 1e3 (MPMJello.py:12) stays bounded.  The c0 workload uses 1e3."""
+    from mpm_cuda_b200 import scenes as S
+    from helpers import oracle_for
+    stiff = oracle_for(S.c0_jello2d(E=1e4))
+    assert any(stiff.step(1) != 0 for _ in range(120))
+    soft = oracle_for(S.c0_jello2d())
+    assert all(soft.step(1) == 0 for _ in range(300))
+    assert float(np.abs(soft.state()["v"]).max()) < 5.0
