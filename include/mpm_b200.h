@@ -142,6 +142,13 @@ typedef struct mpm_options {
     int kernel_config;  /* fused-kernel launch configuration (chunk size and
                            CTAs per SM, see mpm_num_kernel_configs); -1 =
                            choose with the autotuner at creation */
+    int adaptive_dt;    /* MPM_P2G_ATOMIC only: each scene's dt becomes its
+                           largest; every substep picks the next from the CFL
+                           bound cfl * h / max(|v| + material wave speed), on
+                           the device inside the substep graph (the reference
+                           computes a dt factor it never applies,
+                           MPMCUDA.cu:915-920).  Default 0 (fixed dt). */
+    float cfl;          /* CFL number of adaptive dt, (0, 1]; default 0.5 */
 } mpm_options;
 
 typedef struct mpm_handle mpm_handle;
@@ -213,6 +220,11 @@ int mpm_get_grid(mpm_handle *h, int scene, float *mass, float *vel);
 /* Simulated time and substep count of a scene (the reference's public
  * current_time / current_frame, MPMSimulator.cuh:86-87). */
 int mpm_get_time(mpm_handle *h, double *current_time, int64_t *current_frame);
+
+/* Simulated time and current dt of one scene.  With adaptive dt each scene
+ * has its own clock, kept on the device (this call waits for the stream);
+ * mpm_get_time then reports scene 0's. */
+int mpm_get_scene_time(mpm_handle *h, int scene, double *time, float *dt);
 
 /* Replaces OutputBego(path, positions) (src/utilities/FilesIO.h:10,
  * FilesIO.cpp:6-24): writes the scene's positions as a Houdini .bgeo

@@ -48,7 +48,7 @@ class SceneDesc(C.Structure):
 class Options(C.Structure):
     _fields_ = [("p2g_mode", C.c_int), ("stress_mode", C.c_int), ("use_graph", C.c_int),
                 ("block_threads", C.c_int), ("device", C.c_int), ("rebin_interval", C.c_int),
-                ("kernel_config", C.c_int)]
+                ("kernel_config", C.c_int), ("adaptive_dt", C.c_int), ("cfl", C.c_float)]
 
 
 class SurrogateTrainOptions(C.Structure):
@@ -78,6 +78,7 @@ EXPORTS = {
     "mpm_set_state": (C.c_int, [C.c_void_p, C.c_int, _FP, _FP, _FP, _FP, _FP]),
     "mpm_get_grid": (C.c_int, [C.c_void_p, C.c_int, _FP, _FP]),
     "mpm_get_time": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "mpm_get_scene_time": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_float)]),
     "mpm_write_bgeo": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p]),
     "mpm_write_bgeo_positions": (C.c_int, [C.c_char_p, _FP, C.c_int64]),
     "mpm_set_p2g_mode": (C.c_int, [C.c_void_p, C.c_int]),

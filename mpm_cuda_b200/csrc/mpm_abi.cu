@@ -53,6 +53,8 @@ void mpm_default_options(mpm_options* opt) {
     if (!opt) return;
     opt->p2g_mode = MPM_P2G_ATOMIC;
     opt->stress_mode = MPM_STRESS_PLAIN;
+    opt->adaptive_dt = 0;
+    opt->cfl = 0.5f;
     opt->use_graph = 1;
     opt->block_threads = 0;
     opt->device = 0;
@@ -227,9 +229,18 @@ int mpm_autotune(mpm_handle* h, int n_substeps, int* chosen, float* ms_per_subst
 
 int mpm_get_time(mpm_handle* h, double* t, int64_t* frame) {
     if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_get_time: NULL handle");
-    if (t) *t = h->eng.current_time;
     if (frame) *frame = h->eng.current_frame;
+    if (!t) return MPM_OK;
+    if (h->eng.opt.adaptive_dt) return h->eng.scene_time_of(0, t, nullptr);
+    *t = h->eng.current_time;
     return MPM_OK;
+}
+
+int mpm_get_scene_time(mpm_handle* h, int scene, double* t, float* dt) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_get_scene_time: NULL handle");
+    if (scene < 0 || scene >= (int)h->eng.scenes_h.size())
+        return fail(h, MPM_ERR_INVALID, "mpm_get_scene_time: scene %d out of range", scene);
+    return h->eng.scene_time_of(scene, t, dt);
 }
 
 int mpm_write_bgeo(mpm_handle* h, int scene, const char* path) {

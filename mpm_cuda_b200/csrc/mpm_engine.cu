@@ -107,6 +107,14 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
         msg = "mpm_create: bad p2g_mode";
         return MPM_ERR_INVALID;
     }
+    if (opt.adaptive_dt && opt.p2g_mode != MPM_P2G_ATOMIC) {
+        msg = "mpm_create: adaptive dt runs in MPM_P2G_ATOMIC only";
+        return MPM_ERR_UNSUPPORTED;
+    }
+    if (opt.adaptive_dt && !(opt.cfl > 0.f && opt.cfl <= 1.f)) {
+        msg = "mpm_create: cfl must be in (0, 1]";
+        return MPM_ERR_INVALID;
+    }
     if (opt.stress_mode != MPM_STRESS_PLAIN) {
         msg = "mpm_create: select the surrogate stress with mpm_set_stress_mode after creation";
         return MPM_ERR_UNSUPPORTED;
@@ -194,6 +202,7 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
         block_off += sp.n_blocks;
         scenes_h[s] = sp;
         scene_begin[s] = p_off;
+        double signal = 0.0;
         for (int gi = 0; gi < d.n_groups; ++gi) {
             const mpm_group_desc& g = d.groups[gi];
             const mpm_material_desc& m = g.material;
@@ -211,10 +220,31 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
             gp.gamma = (float)m.gamma;
             gp.p_mass = (float)g.p_mass;
             gp.p_vol = (float)g.p_vol;
+            const double rho = g.p_mass / g.p_vol;
+            gp.wave = (float)(m.type == MPM_WATER ? std::sqrt(m.bulk_k * m.gamma / rho) : std::sqrt((la + 2.0 * mu) / rho));
             groups_h.push_back(gp);
             p_off += g.n;
+            // fastest initial signal of the scene: wave speed + initial velocity
+            double v0 = std::sqrt(g.init_v[0] * g.init_v[0] + g.init_v[1] * g.init_v[1] + g.init_v[2] * g.init_v[2]);
+            if (g.v)
+                for (int64_t k = 0; k < g.n; ++k) {
+                    double vv = 0.0;
+                    for (int a = 0; a < dim; ++a) vv += (double)g.v[k * dim + a] * g.v[k * dim + a];
+                    v0 = std::max(v0, std::sqrt(vv));
+                }
+            signal = std::max(signal, gp.wave + v0);
         }
         scene_count[s] = p_off - scene_begin[s];
+        // adaptive dt: the scene's dt is the largest; the first substep takes the
+        // CFL bound of the initial signal speed
+        SceneParams& sq = scenes_h[s];
+        sq.adaptive = opt.adaptive_dt ? 1 : 0;
+        sq.cfl = opt.cfl;
+        sq.dt_max = sq.dt;
+        sq.dt_min = sq.dt * 1e-4f;
+        if (opt.adaptive_dt && signal > 0.0)
+            sq.dt = (float)std::max((double)sq.dt_min, std::min((double)sq.dt_max, opt.cfl * sq.h / signal));
+        sq.dt_next = sq.dt;
     }
     if (block_off > 0x7fffffffLL) return bad(MPM_ERR_INVALID, "mpm_create: grids too large");
     total_blocks = block_off;
@@ -300,6 +330,8 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     if ((rc = alloc((void**)&active, total_blocks * sizeof(int), "active")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&blk_epoch, total_blocks * sizeof(int), "blk_epoch")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&counters, CNT_N * sizeof(int), "counters")) != MPM_OK) return rc;
+    if ((rc = alloc((void**)&speed_max, scenes_h.size() * sizeof(unsigned), "speed maxima")) != MPM_OK) return rc;
+    if ((rc = alloc((void**)&scene_time, scenes_h.size() * sizeof(double), "scene times")) != MPM_OK) return rc;
     list_cap = cap / kFusedCfgs[kNumFusedCfgs - 1].chunk + std::min<long long>(cap, total_blocks) + 1;
     if ((rc = alloc((void**)&chunks, kMats * list_cap * sizeof(Chunk), "chunks")) != MPM_OK) return rc;
     key_bits = 12;
@@ -347,6 +379,8 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     if (e == cudaSuccess) e = cudaMemset(seg_count, 0, total_blocks * 4 * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(blk_epoch, 0xff, total_blocks * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(counters, 0, CNT_N * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(speed_max, 0, scenes_h.size() * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(scene_time, 0, scenes_h.size() * sizeof(double));
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         msg = std::string("mpm_create: upload: ") + cudaGetErrorString(e);
@@ -458,6 +492,13 @@ int Engine::autotune(int steps, float* best_ms) {
     if (e == cudaSuccess) e = cudaMemcpy(bk_id, ids[cur], cap * sizeof(uint32_t), cudaMemcpyDeviceToDevice);
     const double t0 = current_time;
     const long long f0 = current_frame;
+    // adaptive dt changes the scene table and the scene times: restore them too
+    std::vector<SceneParams> bk_scenes(scenes_h.size());
+    std::vector<double> bk_time(scenes_h.size());
+    if (e == cudaSuccess)
+        e = cudaMemcpy(bk_scenes.data(), scenes_d, bk_scenes.size() * sizeof(SceneParams), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(bk_time.data(), scene_time, bk_time.size() * sizeof(double), cudaMemcpyDeviceToHost);
     const int mode0 = opt.p2g_mode;
     opt.p2g_mode = MPM_P2G_ATOMIC;
     int best = cfg;
@@ -468,6 +509,9 @@ int Engine::autotune(int steps, float* best_ms) {
     if (e == cudaSuccess) e = cudaEventCreate(&b);
     for (int ci = 0; ci < kNumFusedCfgs && e == cudaSuccess && rc == MPM_OK; ++ci) {
         e = cudaMemcpyAsync(st[cur], bk_state, state_bytes, cudaMemcpyDeviceToDevice, stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(scenes_d, bk_scenes.data(), bk_scenes.size() * sizeof(SceneParams),
+                                cudaMemcpyHostToDevice, stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(gp[cur], bk_grp, cap * sizeof(uint16_t), cudaMemcpyDeviceToDevice, stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(ids[cur], bk_id, cap * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream);
         if (e != cudaSuccess) break;
@@ -493,6 +537,11 @@ int Engine::autotune(int steps, float* best_ms) {
     if (e == cudaSuccess) e = cudaMemcpy(ids[cur], bk_id, cap * sizeof(uint32_t), cudaMemcpyDeviceToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(err_d, &err_before, sizeof(unsigned), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(counters + CNT_FALLBACK, 0, 2 * sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(scenes_d, bk_scenes.data(), bk_scenes.size() * sizeof(SceneParams), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(scene_time, bk_time.data(), bk_time.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(speed_max, 0, scenes_h.size() * sizeof(unsigned));
     cudaFree(bk_state);
     cudaFree(bk_grp);
     cudaFree(bk_id);
@@ -533,7 +582,7 @@ void Engine::release() {
     }
     void* ptrs[] = {groups_d, scenes_d, grid_mom, grid_vel, err_d, keys[0], keys[1], vals[0], vals[1],
                     cell_count, seg_count, seg_start, sort_tmp, blk_flag, active, blk_epoch, counters, chunks,
-                    scan_tmp, pos_out, cell_end, det_src, sur_counts};
+                    scan_tmp, pos_out, cell_end, det_src, sur_counts, speed_max, scene_time};
     for (void* p : ptrs) cudaFree(p);
     groups_d = nullptr;
     scenes_d = nullptr;
@@ -559,6 +608,8 @@ void Engine::release() {
     if (copy_stream) cudaStreamDestroy(copy_stream);
     copy_stream = nullptr;
     sur_counts = nullptr;
+    speed_max = nullptr;
+    scene_time = nullptr;
     sur = nullptr;
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
@@ -675,6 +726,7 @@ FusedArgs Engine::fused_args(int mat, bool bump) {
     A.bump_epoch = bump ? 1 : 0;
     A.err_word = err_d;
     A.fallback = (unsigned*)(counters + CNT_FALLBACK);
+    A.speed_max = opt.adaptive_dt ? speed_max : nullptr;
     return A;
 }
 
@@ -715,6 +767,14 @@ void Engine::enqueue_g2p2g(int parity) {
 void Engine::enqueue_fused_substep(int parity) {
     enqueue_grid_update();
     enqueue_g2p2g(parity);
+    enqueue_adapt_dt();
+}
+
+void Engine::enqueue_adapt_dt() {
+    if (!opt.adaptive_dt) return;
+    const int n_scenes = (int)scenes_h.size();
+    k_adapt_dt<<<(n_scenes + 127) / 128, 128, 0, stream>>>(scenes_d, n_scenes, speed_max, scene_time);
+    note_launch("k_adapt_dt");
 }
 
 // deterministic P2G of the current state into grid_mom (blocks marked active)
@@ -1158,6 +1218,10 @@ int Engine::bin_stats(int64_t* fallbacks, int64_t* rebins) {
 }
 
 int Engine::set_p2g_mode(int mode) {
+    if (opt.adaptive_dt && mode != MPM_P2G_ATOMIC) {
+        last_error = "mpm_set_p2g_mode: adaptive dt runs in MPM_P2G_ATOMIC only";
+        return MPM_ERR_UNSUPPORTED;
+    }
     if (sur && mode != MPM_P2G_ATOMIC) {
         last_error = "mpm_set_p2g_mode: the surrogate stress runs in MPM_P2G_ATOMIC only";
         return MPM_ERR_UNSUPPORTED;
@@ -1215,6 +1279,25 @@ int Engine::sur_refresh() {
     return MPM_OK;
 }
 
+// simulated time and current substep of a scene: with adaptive dt the device
+// owns the clock (k_adapt_dt), otherwise substeps x dt
+int Engine::scene_time_of(int scene, double* t, float* dt) {
+    if (!opt.adaptive_dt) {
+        if (t) *t = (double)current_frame * scenes_h[scene].dt;
+        if (dt) *dt = scenes_h[scene].dt;
+        return MPM_OK;
+    }
+    MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
+    if (t) MPM_CUDA_TRY(cudaMemcpy(t, scene_time + scene, sizeof(double), cudaMemcpyDeviceToHost), "time download");
+    if (dt) {
+        SceneParams sp;
+        MPM_CUDA_TRY(cudaMemcpy(&sp, scenes_d + scene, sizeof(sp), cudaMemcpyDeviceToHost), "scene download");
+        *dt = sp.dt;
+    }
+    return MPM_OK;
+}
+
 int Engine::stress_stats(int64_t* net, int64_t* fallback) {
     MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
     MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
@@ -1258,6 +1341,7 @@ int Engine::profile_stages(int n, float* out_ms, int n_out, int* n_written) {
             enqueue_grid_update();
             cudaEventRecord(ev[1], stream);
             enqueue_g2p2g(cur);
+            enqueue_adapt_dt();
             cudaEventRecord(ev[2], stream);
             cudaEventSynchronize(ev[2]);
             float a = 0.f, b = 0.f;

@@ -91,6 +91,10 @@ struct Engine {
     long long sur_version = -1;
     int sur_ctas[3] = {0, 0, 0};
     unsigned long long* sur_counts = nullptr;
+    // adaptive dt: per scene max signal speed of the last pass (float bits) and
+    // simulated time (the device owns the clock when dt adapts)
+    unsigned* speed_max = nullptr;
+    double* scene_time = nullptr;
     int update_ctas = 0;
     int steps_since_rebin = 0;
 
@@ -117,6 +121,7 @@ struct Engine {
     int set_p2g_mode(int mode);
     int set_stress_mode(int mode, Surrogate* s);
     int stress_stats(int64_t* net, int64_t* fallback);
+    int scene_time_of(int scene, double* t, float* dt);
     int profile_stages(int n, float* out_ms, int n_out, int* n_written);
     int get_positions(int scene, float* out);
     int get_positions_async(int scene, float* out, long long* ticket);
@@ -135,6 +140,7 @@ struct Engine {
     void enqueue_rebin(int from);
     void enqueue_fused_substep(int parity);
     void enqueue_grid_update();
+    void enqueue_adapt_dt();
     void enqueue_g2p2g(int parity);
     FusedArgs fused_args(int mat, bool bump);
     int prologue();

@@ -256,6 +256,7 @@ struct FusedArgs {
     int bump_epoch;
     unsigned* err_word;
     unsigned* fallback;  // count of particles that used global memory
+    unsigned* speed_max; // adaptive dt: per scene max of |v| + wave (float bits); null when off
 };
 
 template <int D>
@@ -427,16 +428,46 @@ __device__ __forceinline__ void mark_touched(unsigned touched, const SceneParams
     }
 }
 
+// Per-CTA maximum of the particles' signal speed |v| + wave for adaptive dt:
+// warps reduce into a shared word during a chunk, thread 0 folds it into a
+// running maximum of the current scene after the chunk and sends one global
+// atomicMax when the scene changes and at the end (chunks are ordered by block,
+// so a CTA meets few scene changes and the global word sees few atomics).
+__device__ __forceinline__ void speed_warp_reduce(unsigned bits, unsigned* shared_word) {
+    bits = __reduce_max_sync(0xffffffffu, bits);
+    if ((threadIdx.x & 31) == 0 && bits) atomicMax(shared_word, bits);
+}
+struct SpeedFlush {
+    int scene = -1;
+    unsigned best = 0u;
+    __device__ __forceinline__ void fold(int si, unsigned* shared_word, unsigned* global_max) {
+        if (threadIdx.x != 0 || !global_max) return;
+        const unsigned v = *shared_word;
+        *shared_word = 0u;
+        if (si != scene) {
+            if (scene >= 0 && best) atomicMax(&global_max[scene], best);
+            scene = si;
+            best = v;
+        } else {
+            best = max(best, v);
+        }
+    }
+    __device__ __forceinline__ void flush(unsigned* global_max) {
+        if (threadIdx.x == 0 && global_max && scene >= 0 && best) atomicMax(&global_max[scene], best);
+    }
+};
+
 // Persistent loop of a CTA over a material's chunk list.  Chunks come from a
 // global cursor (chunk sizes vary); the index of the chunk after next and the
 // next chunk's velocity window are fetched while the current chunk is
 // processed, so the cursor atomic and the window's L2 round trips are off the
 // critical path.  body(ch, sc, o, tv, touched) runs with chunk ch's window in
-// tv; every thread of the CTA calls it.  Three barriers per chunk: window
-// landed, body done (touched complete, window free), loop state published.
-template <int D, int NT, class Body>
+// tv; every thread of the CTA calls it; post(scene index) runs after the
+// body's barrier.  Three barriers per chunk: window landed, body done (touched
+// complete, window free), loop state published.
+template <int D, int NT, class Body, class Post>
 __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][TileShape<D>::VN],
-                                           unsigned (&touched)[2], int (&s_cn)[2], Body body) {
+                                           unsigned (&touched)[2], int (&s_cn)[2], Body body, Post post) {
     const int nch = *A.n_chunks;
     if (threadIdx.x == 0) {
         s_cn[0] = atomicAdd(A.cursor, 1);
@@ -458,12 +489,14 @@ __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][T
         cp_async_wait<1>();  // this thread's copies of the current window
         __syncthreads();     // everyone's
         const Chunk ch = A.chunks[cur];
-        const SceneParams& sc = A.scenes[scene_of_block(A.scenes, A.n_scenes, ch.block)];
+        const int si = scene_of_block(A.scenes, A.n_scenes, ch.block);
+        const SceneParams& sc = A.scenes[si];
         int o[3];
         tile_origin<D>(sc, ch.block - sc.block_off, o);
         body(ch, sc, o, tv[b], &touched[b]);
         __syncthreads();
         mark_touched<D>(touched[b], sc, o, A);
+        post(si);
         if (threadIdx.x == 0) {
             s_cn[0] = nxt;
             s_cn[1] = after;
@@ -488,39 +521,67 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
     __shared__ __align__(16) float4 tv[2][TS::VN];  // grid velocity windows (double-buffered)
     __shared__ unsigned touched[2];                 // 3^D neighbour-block bits
     __shared__ int s_cn[2];
+    __shared__ unsigned s_speed;                    // adaptive dt: this chunk's max signal speed
 
     if (A.bump_epoch && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.epoch, 1);
+    if (threadIdx.x == 0) s_speed = 0u;
+    SpeedFlush speed;
     chunk_loop<D, CHUNK>(A, tv, touched, s_cn,
                          [&](const Chunk& ch, const SceneParams& sc, const int* o, const float4* w, unsigned* tb) {
-        if ((int)threadIdx.x >= ch.count) return;
-        const long long i = (long long)ch.start + threadIdx.x;
-        float* S = pb.s;
-        const long long cap = pb.cap;
-        unsigned err = 0;
-        float x[D];
+        unsigned speed_bits = 0u;
+        if ((int)threadIdx.x < ch.count) {
+            const long long i = (long long)ch.start + threadIdx.x;
+            float* S = pb.s;
+            const long long cap = pb.cap;
+            unsigned err = 0;
+            float x[D];
 #pragma unroll
-        for (int a = 0; a < D; ++a) x[a] = S[(P::X + a) * cap + i];
-        Stencil<D> st;
-        if (make_stencil<D>(x, sc, st, err)) {
-            G2PAcc<D> acc;
-            g2p_window<D>(st, o, w, sc, A, acc);
-            // loaded after the gather, its register peak
-            const GroupParams g = A.groups[pb.grp[i]];
-            float F[D * D], Cn[D * D], v[D], aux;
-            ElasticSVD<D> esvd;  // snow: the plasticity step's decomposition, reused by the stress
-            err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux, MAT == SNOW ? &esvd : nullptr);
+            for (int a = 0; a < D; ++a) x[a] = S[(P::X + a) * cap + i];
+            Stencil<D> st;
+            if (make_stencil<D>(x, sc, st, err)) {
+                G2PAcc<D> acc;
+                g2p_window<D>(st, o, w, sc, A, acc);
+                // loaded after the gather, its register peak
+                const GroupParams g = A.groups[pb.grp[i]];
+                float F[D * D], Cn[D * D], v[D], aux;
+                ElasticSVD<D> esvd;  // snow: the plasticity step's decomposition, reused by the stress
+                err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux,
+                                                MAT == SNOW ? &esvd : nullptr);
+                if (A.speed_max) speed_bits = __float_as_uint(signal_speed<D, MAT>(v, g, aux));
 
-            // ---- stress + P2G of the next substep
-            Stencil<D> sn;
-            if (make_stencil<D>(x, sc, sn, err)) {
-                P2GSource<D> src;
-                if (MAT == SNOW) snow_stress_source<D>(v, Cn, esvd, aux, g, sc, src);
-                else particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc, src);
-                scatter_global<D>(sn, src, sc, o, A, tb);
+                // ---- stress + P2G of the next substep (its dt is dt_next)
+                Stencil<D> sn;
+                if (make_stencil<D>(x, sc, sn, err)) {
+                    P2GSource<D> src;
+                    if (MAT == SNOW) snow_stress_source<D>(v, Cn, esvd, aux, g, sc.dt_next, src);
+                    else particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc.dt_next, src);
+                    scatter_global<D>(sn, src, sc, o, A, tb);
+                }
             }
+            if (err) atomicOr(A.err_word, err);
         }
-        if (err) atomicOr(A.err_word, err);
-    });
+        if (A.speed_max) speed_warp_reduce(speed_bits, &s_speed);
+    }, [&](int si) { speed.fold(si, &s_speed, A.speed_max); });
+    speed.flush(A.speed_max);
+}
+
+// Adaptive dt, once per substep after the fused pass (one thread per scene):
+// the substep that ran advances the scene's time; the next one uses the dt its
+// P2G was built with; the one after gets clamp(cfl h / max(|v| + wave),
+// dt_min, dt_max) from the speeds this pass saw.  (The reference computes a
+// max(J, 1/J)^3 factor for this and never applies it, MPMCUDA.cu:915-920.)
+static __global__ void k_adapt_dt(SceneParams* scenes, int n_scenes, unsigned* speed_max, double* scene_time) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_scenes) return;
+    SceneParams& sc = scenes[s];
+    scene_time[s] += (double)sc.dt;
+    const float v = __uint_as_float(speed_max[s]);
+    speed_max[s] = 0u;
+    float dtn = sc.dt_max;
+    if (v > 0.f) dtn = fminf(dtn, sc.cfl * sc.h / v);
+    dtn = fmaxf(dtn, sc.dt_min);
+    sc.dt = sc.dt_next;
+    sc.dt_next = dtn;
 }
 
 }  // namespace mpm

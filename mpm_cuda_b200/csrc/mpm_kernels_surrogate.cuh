@@ -43,6 +43,7 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
     extern __shared__ float sxy[];                  // CHUNK rows: network inputs, then outputs
     __shared__ unsigned touched[2];
     __shared__ int s_cn[2];
+    __shared__ unsigned s_speed;  // adaptive dt: this chunk's max signal speed
 
     if (A.bump_epoch && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.epoch, 1);
     {
@@ -52,6 +53,8 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
     }  // published by the first barrier of chunk_loop
     const int lane = threadIdx.x & 31, w0 = threadIdx.x & ~31;
     unsigned n_net = 0, n_svd = 0;
+    if (threadIdx.x == 0) s_speed = 0u;
+    SpeedFlush speed;
     chunk_loop<D, CHUNK>(A, tv, touched, s_cn,
                          [&](const Chunk& ch, const SceneParams& sc, const int* o, const float4* w, unsigned* tb) {
         const long long i = (long long)ch.start + threadIdx.x;
@@ -61,6 +64,7 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
         bool next = false;      // the particle scatters into the next substep
         bool eligible = false;  // its group takes the network's stress
         int gi = 0;             // its group (re-read after the network: fewer live registers)
+        unsigned speed_bits = 0u;
         float* row = sxy + threadIdx.x * XS;
         if ((int)threadIdx.x < ch.count) {
             gi = pb.grp[i];
@@ -74,6 +78,7 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
                 const GroupParams g = A.groups[gi];
                 float F[D * D], Cn[D * D], v[D], aux;
                 err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux);
+                if (A.speed_max) speed_bits = __float_as_uint(signal_speed<D, MAT>(v, g, aux));
                 Stencil<D> sn;
                 next = make_stencil<D>(x, sc, sn, err);
                 eligible = next && g.surrogate != 0;
@@ -116,16 +121,18 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
             }
             P2GSource<D> src;
             if (use) {
-                source_from_tau<D>(v, Cn, tau, g, sc, src);
+                source_from_tau<D>(v, Cn, tau, g, sc.dt_next, src);
                 ++n_net;
             } else {
-                particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc, src);
+                particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc.dt_next, src);
                 ++n_svd;
             }
             scatter_global<D>(sn, src, sc, o, A, tb);
         }
         if (err) atomicOr(A.err_word, err);
-    });
+        if (A.speed_max) speed_warp_reduce(speed_bits, &s_speed);
+    }, [&](int si) { speed.fold(si, &s_speed, A.speed_max); });
+    speed.flush(A.speed_max);
     n_net = __reduce_add_sync(0xffffffffu, n_net);
     n_svd = __reduce_add_sync(0xffffffffu, n_svd);
     if (lane == 0 && (n_net | n_svd)) {

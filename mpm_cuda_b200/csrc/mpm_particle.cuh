@@ -86,8 +86,8 @@ __device__ __forceinline__ bool is_mat(const GroupParams& g, int m) {
 
 template <int D, int MAT = -1>
 __device__ __forceinline__ void particle_stress_source(const float* v, const float* C, const float* F,
-                                                       float aux, const GroupParams& g,
-                                                       const SceneParams& sc, P2GSource<D>& src) {
+                                                       float aux, const GroupParams& g, float dt,
+                                                       P2GSource<D>& src) {
     float tau[D * D];
     if (is_mat<MAT>(g, WATER)) {
         // p = K (J^-gamma - 1) (MPMCUDA.cu:353, MPMWater.py:92); tau_eff = -p J I
@@ -105,7 +105,7 @@ __device__ __forceinline__ void particle_stress_source(const float* v, const flo
         }
         kirchhoff_fcr<D>(F, mu, la, tau);
     }
-    const float k = -sc.dt * g.p_vol;
+    const float k = -dt * g.p_vol;
 #pragma unroll
     for (int i = 0; i < D * D; ++i) {
         src.A[i] = k * tau[i];
@@ -114,6 +114,14 @@ __device__ __forceinline__ void particle_stress_source(const float* v, const flo
 #pragma unroll
     for (int a = 0; a < D; ++a) src.mv[a] = g.p_mass * v[a];
     src.m = g.p_mass;
+}
+
+// the same with the scene's current substep
+template <int D, int MAT = -1>
+__device__ __forceinline__ void particle_stress_source(const float* v, const float* C, const float* F,
+                                                       float aux, const GroupParams& g, const SceneParams& sc,
+                                                       P2GSource<D>& src) {
+    particle_stress_source<D, MAT>(v, C, F, aux, g, sc.dt, src);
 }
 
 // Left singular vectors and clamped singular values of snow's new elastic F
@@ -131,8 +139,7 @@ struct ElasticSVD {
 // (MPMCUDA.cu:342-347) and the fixed-corotated stress of U, s.
 template <int D>
 __device__ __forceinline__ void snow_stress_source(const float* v, const float* C, const ElasticSVD<D>& e,
-                                                   float aux, const GroupParams& g, const SceneParams& sc,
-                                                   P2GSource<D>& src) {
+                                                   float aux, const GroupParams& g, float dt, P2GSource<D>& src) {
     const float hc = expf(g.xi * (1.f - aux));
     const float mu = g.mu * hc, la = g.lambda * hc;
     float J = 1.f, dg[D];
@@ -142,7 +149,7 @@ __device__ __forceinline__ void snow_stress_source(const float* v, const float* 
         dg[k] = 2.f * mu * e.s[k] * (e.s[k] - 1.f);
     }
     const float iso = la * J * (J - 1.f);
-    const float kf = -sc.dt * g.p_vol;
+    const float kf = -dt * g.p_vol;
 #pragma unroll
     for (int i = 0; i < D; ++i)
 #pragma unroll
@@ -161,8 +168,8 @@ __device__ __forceinline__ void snow_stress_source(const float* v, const float* 
 // the same source from a given Kirchhoff stress (the surrogate path)
 template <int D>
 __device__ __forceinline__ void source_from_tau(const float* v, const float* C, const float* tau, const GroupParams& g,
-                                                const SceneParams& sc, P2GSource<D>& src) {
-    const float k = -sc.dt * g.p_vol;
+                                                float dt, P2GSource<D>& src) {
+    const float k = -dt * g.p_vol;
 #pragma unroll
     for (int i = 0; i < D * D; ++i) {
         src.A[i] = k * tau[i];
@@ -439,6 +446,19 @@ __device__ __forceinline__ void p2g_scatter(const Stencil<D>& st, const P2GSourc
             }
         }
     }
+}
+
+// |v| plus the material's signal speed, for adaptive dt.  Snow's hardening
+// scales its stiffness by exp(xi (1 - Jp)), so its wave speed by the square
+// root of that.
+template <int D, int MAT>
+__device__ __forceinline__ float signal_speed(const float* v, const GroupParams& g, float aux) {
+    float vv = 0.f;
+#pragma unroll
+    for (int a = 0; a < D; ++a) vv = fmaf(v[a], v[a], vv);
+    float c = g.wave;
+    if (MAT == SNOW) c *= expf(0.5f * g.xi * (1.f - aux));
+    return sqrtf(vv) + c;
 }
 
 // Material update after G2P (MPMCUDA.cu:588-713, MPMSnow.py:135-150,

@@ -21,6 +21,8 @@ struct GroupParams {
     float bulk_k, gamma;
     float p_mass, p_vol;
     int surrogate;  // stress from the learned surrogate (MPM_STRESS_SURROGATE)
+    float wave;     // signal speed of the material at rest: sqrt((lambda + 2 mu) / rho)
+                    // for solids, sqrt(K gamma / rho) for water (adaptive dt)
 };
 
 // One scene's grid and integration constants (Grid, MPMSimulator.cuh:54-64).
@@ -29,7 +31,7 @@ struct SceneParams {
     int dim;
     float h, inv_h;
     float origin[3];
-    float dt;
+    float dt;  // current substep (grid update, G2P, advection)
     float gravity[3];
     int bc_type, bc_lo, bc_hi;
     float mass_eps;
@@ -37,9 +39,12 @@ struct SceneParams {
     long long n_nodes;
     // 4^3 (or 4^2) node blocks: blocks per axis and first block index
     int nb[3];
-    int pad;
+    float dt_next;  // next substep: the fused pass's P2G for it (equal to dt unless adaptive)
     long long block_off;
     long long n_blocks;
+    // adaptive dt (MPM_P2G_ATOMIC): dt_next = clamp(cfl h / max(|v| + wave), dt_min, dt_max)
+    float dt_max, dt_min, cfl;
+    int adaptive;
 };
 
 // Particle state: component planes of one FP32 buffer, plane stride `cap`.

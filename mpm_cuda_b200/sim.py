@@ -133,7 +133,8 @@ class Simulation:
 
     def __init__(self, scenes: Sequence[Scene], p2g_mode: int = L.P2G_ATOMIC,
                  stress_mode: int = L.STRESS_PLAIN, use_graph: bool = True, device: int = 0,
-                 rebin_interval: int = 0, kernel_config: int = -1):
+                 rebin_interval: int = 0, kernel_config: int = -1, adaptive_dt: bool = False,
+                 cfl: float = 0.5):
         lib = L.load()
         self.scenes = list(scenes)
         self.dim = self.scenes[0].dim
@@ -144,6 +145,8 @@ class Simulation:
         opt.p2g_mode, opt.stress_mode, opt.use_graph, opt.device = p2g_mode, stress_mode, int(use_graph), device
         opt.rebin_interval = rebin_interval
         opt.kernel_config = kernel_config
+        opt.adaptive_dt = int(adaptive_dt)
+        opt.cfl = cfl
         h = C.c_void_p()
         L.check(lib.mpm_create(sdescs, len(self.scenes), C.byref(opt), C.byref(h)))
         self._h = h
@@ -215,6 +218,12 @@ class Simulation:
         a, b = C.c_int64(), C.c_int64()
         self._check(self._lib.mpm_get_stress_stats(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def scene_time(self, scene: int = 0):
+        """(simulated time, current dt) of one scene."""
+        t, dt = C.c_double(), C.c_float()
+        self._check(self._lib.mpm_get_scene_time(self._h, scene, C.byref(t), C.byref(dt)))
+        return t.value, dt.value
 
     def time(self):
         t, f = C.c_double(), C.c_int64()

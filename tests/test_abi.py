@@ -38,7 +38,7 @@ def test_struct_sizes_match_header_layout():
     # natural alignment of the C structs in include/mpm_b200.h
     assert C.sizeof(L.MaterialDesc) == 8 + 8 * 8
     assert C.sizeof(L.GroupDesc) == 72 + 16 + 8 + 16 + 24 + 24
-    assert C.sizeof(L.Options) == 28
+    assert C.sizeof(L.Options) == 36
 
 
 def _mk(**kw):
