@@ -226,6 +226,41 @@ int mpm_get_time(mpm_handle *h, double *current_time, int64_t *current_frame);
  * mpm_get_time then reports scene 0's. */
 int mpm_get_scene_time(mpm_handle *h, int scene, double *time, float *dt);
 
+/* ------------------------------------------------------------------------
+ * Particle seeding on the GPU.  Replaces the reference's host loop
+ * (MPMSimulator.cpp:198-257): every cell of the lattice origin + i h that the
+ * object's world bounding box touches gets ppc samples at hashed positions
+ * inside the cell (deterministic for a seed; the reference uses rand()), and
+ * the samples inside the object are kept, in cell order.  Objects are unit
+ * shapes centred at the origin, or a closed triangle mesh (inside test by
+ * ray-crossing parity), placed by world = translation + scale * (R local)
+ * (the reference's model matrix translate * scale * rotate, model.cpp:202-207).
+ * ---------------------------------------------------------------------- */
+enum mpm_shape {
+    MPM_SHAPE_CUBE = 0,     /* [-1/2, 1/2]^3 */
+    MPM_SHAPE_SPHERE = 1,   /* ball of radius 1/2 */
+    MPM_SHAPE_CYLINDER = 2, /* radius 1/2, height 1 along y */
+    MPM_SHAPE_MESH = 3      /* vertices / triangles below (3D only) */
+};
+
+typedef struct mpm_seed_object {
+    int shape;              /* enum mpm_shape */
+    double rotation[9];     /* R, row-major */
+    double scale[3];
+    double translation[3];
+    const float *vertices;  /* MPM_SHAPE_MESH: n_vertices x 3, local coordinates */
+    int64_t n_vertices;
+    const int32_t *triangles; /* n_triangles x 3 vertex indices */
+    int64_t n_triangles;
+} mpm_seed_object;
+
+/* Seeds one object with ppc (1..64) samples per lattice cell of spacing h
+ * anchored at origin (NULL = 0) in dim 2 or 3.  *n receives the particle
+ * count; with host_out (cap floats, >= n * dim) the positions are written
+ * too, so a first call with host_out = NULL sizes the buffer. */
+int mpm_seed(const mpm_seed_object *obj, int dim, double h, const double *origin, int ppc,
+             uint64_t seed, int device, float *host_out, size_t cap, int64_t *n);
+
 /* Replaces OutputBego(path, positions) (src/utilities/FilesIO.h:10,
  * FilesIO.cpp:6-24): writes the scene's positions as a Houdini .bgeo
  * particle file with one float[3] "position" attribute. */

@@ -16,18 +16,17 @@
 //   "builtin:sphere"    the ball of radius 0.5 at the origin
 //   "builtin:cylinder"  radius 0.5, height 1 along y, centred at the origin
 //   anything else       a Wavefront .obj file (v / f records), closed mesh,
-//                       inside test by ray-crossing parity
+//                       inside test by ray-crossing parity (on the GPU)
 // Differences from the reference: particle volume is h^3 / ppc (the reference
 // assigns h^3, MPMSimulator.cpp:252,263; set Options::reference_volume to
-// reproduce it); the random jitter comes from a seeded std::mt19937 instead of
-// rand(); positions are float on the device.
+// reproduce it); the samples are drawn on the GPU by mpm_seed from a seeded
+// counter hash instead of rand(); positions are float on the device.
 #pragma once
 
 #include <array>
 #include <cmath>
 #include <cstdint>
 #include <fstream>
-#include <random>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -105,7 +104,8 @@ inline Mat3 rotation(double deg, vec3 axis) {
     return r;
 }
 
-// closed triangle mesh with a ray-crossing inside test
+// closed triangle mesh (Wavefront .obj v / f records); its inside test runs
+// on the GPU in mpm_seed
 struct Mesh {
     std::vector<double> v;     // xyz
     std::vector<int> tri;      // 3 indices per triangle
@@ -141,32 +141,6 @@ struct Mesh {
                 m.hi[a] = std::max(m.hi[a], m.v[i + a]);
             }
         return m;
-    }
-
-    // parity of crossings of a ray from p along a fixed skew direction
-    // (Moller-Trumbore ray/triangle test)
-    bool inside(const double* p) const {
-        const double d[3] = {0.8729436, 0.3961478, 0.2846573};
-        int hits = 0;
-        for (size_t t = 0; t < tri.size(); t += 3) {
-            const double* a = &v[3 * tri[t]];
-            const double* b = &v[3 * tri[t + 1]];
-            const double* c = &v[3 * tri[t + 2]];
-            const double e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
-            const double e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
-            const double q[3] = {d[1] * e2[2] - d[2] * e2[1], d[2] * e2[0] - d[0] * e2[2], d[0] * e2[1] - d[1] * e2[0]};
-            const double det = e1[0] * q[0] + e1[1] * q[1] + e1[2] * q[2];
-            if (std::fabs(det) < 1e-300) continue;
-            const double inv = 1.0 / det;
-            const double s[3] = {p[0] - a[0], p[1] - a[1], p[2] - a[2]};
-            const double u = (s[0] * q[0] + s[1] * q[1] + s[2] * q[2]) * inv;
-            if (u < 0.0 || u > 1.0) continue;
-            const double r[3] = {s[1] * e1[2] - s[2] * e1[1], s[2] * e1[0] - s[0] * e1[2], s[0] * e1[1] - s[1] * e1[0]};
-            const double w = (d[0] * r[0] + d[1] * r[1] + d[2] * r[2]) * inv;
-            if (w < 0.0 || u + w > 1.0) continue;
-            if ((e2[0] * r[0] + e2[1] * r[1] + e2[2] * r[2]) * inv > 0.0) ++hits;
-        }
-        return (hits & 1) != 0;
     }
 };
 
@@ -225,14 +199,12 @@ class MPMSimulator {
         mGrid.nodeNumDimX = nx;
         mGrid.nodeNumDimY = ny;
         mGrid.nodeNumDimZ = nz;
-        std::mt19937 rng(opt.seed);
-        std::uniform_real_distribution<float> U(0.f, 1.f);
         std::vector<std::vector<float>> pos(objs.size());
         std::vector<mpm_group_desc> groups(objs.size());
         const unsigned n[3] = {nx, ny, nz};
         for (size_t k = 0; k < objs.size(); ++k) {
             const ObjInitInfo& o = objs[k];
-            seed_object(o, gap, n, ppc, rng, U, pos[k]);
+            seed_object(o, gap, n, ppc, opt.seed + (unsigned)k, opt.device, pos[k]);
             const Material& m = o.mMaterial;
             mpm_group_desc& g = groups[k];
             g = mpm_group_desc{};
@@ -310,62 +282,58 @@ class MPMSimulator {
         throw std::runtime_error(std::string("mpm_b200: ") + buf);
     }
 
-    static void seed_object(const ObjInitInfo& o, double gap, const unsigned* n, unsigned ppc, std::mt19937& rng,
-                            std::uniform_real_distribution<float>& U, std::vector<float>& out) {
+    // Seeds one object on the GPU (mpm_seed): the object's world bounding box
+    // must lie inside the grid (the reference's checks, MPMSimulator.cpp:214-223)
+    static void seed_object(const ObjInitInfo& o, double gap, const unsigned* n, unsigned ppc, unsigned seed,
+                            int device, std::vector<float>& out) {
         using mpm_shim::Mesh;
         const mpm_shim::Mat3 R = mpm_shim::rotation(o.initRotationDegree, o.initRotationAxis);
-        const double S[3] = {o.initScale.x, o.initScale.y, o.initScale.z};
-        const double T[3] = {o.initTranslation.x, o.initTranslation.y, o.initTranslation.z};
-        int shape = -1;  // 0 cube, 1 sphere, 2 cylinder, 3 mesh
+        mpm_seed_object so{};
+        for (int a = 0; a < 9; ++a) so.rotation[a] = R.m[a];
+        so.scale[0] = o.initScale.x;
+        so.scale[1] = o.initScale.y;
+        so.scale[2] = o.initScale.z;
+        so.translation[0] = o.initTranslation.x;
+        so.translation[1] = o.initTranslation.y;
+        so.translation[2] = o.initTranslation.z;
         Mesh mesh;
+        std::vector<float> verts;
+        std::vector<int32_t> tris;
         double llo[3] = {-0.5, -0.5, -0.5}, lhi[3] = {0.5, 0.5, 0.5};
-        if (o.objPath == "builtin:cube") shape = 0;
-        else if (o.objPath == "builtin:sphere") shape = 1;
-        else if (o.objPath == "builtin:cylinder") shape = 2;
+        if (o.objPath == "builtin:cube") so.shape = MPM_SHAPE_CUBE;
+        else if (o.objPath == "builtin:sphere") so.shape = MPM_SHAPE_SPHERE;
+        else if (o.objPath == "builtin:cylinder") so.shape = MPM_SHAPE_CYLINDER;
         else {
-            shape = 3;
+            so.shape = MPM_SHAPE_MESH;
             mesh = Mesh::load_obj(o.objPath);
+            verts.assign(mesh.v.begin(), mesh.v.end());
+            tris.assign(mesh.tri.begin(), mesh.tri.end());
+            so.vertices = verts.data();
+            so.n_vertices = (int64_t)(verts.size() / 3);
+            so.triangles = tris.data();
+            so.n_triangles = (int64_t)(tris.size() / 3);
             for (int a = 0; a < 3; ++a) {
                 llo[a] = mesh.lo[a];
                 lhi[a] = mesh.hi[a];
             }
         }
         // world bounding box of the transformed local box (model.cpp:202-222)
-        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-        for (int c = 0; c < 8; ++c) {
-            const double p[3] = {(c & 1) ? lhi[0] : llo[0], (c & 2) ? lhi[1] : llo[1], (c & 4) ? lhi[2] : llo[2]};
-            for (int a = 0; a < 3; ++a) {
-                const double w = T[a] + S[a] * (R.m[a * 3] * p[0] + R.m[a * 3 + 1] * p[1] + R.m[a * 3 + 2] * p[2]);
-                lo[a] = std::min(lo[a], w);
-                hi[a] = std::max(hi[a], w);
+        for (int a = 0; a < 3; ++a) {
+            double lo = 1e300, hi = -1e300;
+            for (int c = 0; c < 8; ++c) {
+                const double p[3] = {(c & 1) ? lhi[0] : llo[0], (c & 2) ? lhi[1] : llo[1], (c & 4) ? lhi[2] : llo[2]};
+                const double w = so.translation[a] +
+                                 so.scale[a] * (R.m[a * 3] * p[0] + R.m[a * 3 + 1] * p[1] + R.m[a * 3 + 2] * p[2]);
+                lo = std::min(lo, w);
+                hi = std::max(hi, w);
             }
+            if (lo < 0.0) throw std::runtime_error("ERROR: OBJ lower bound is smaller than grid's origin.");
+            if (hi > (n[a] - 1) * gap) throw std::runtime_error("ERROR: OBJ upper bound is out of the grid.");
         }
-        for (int a = 0; a < 3; ++a) {
-            if (lo[a] < 0.0) throw std::runtime_error("ERROR: OBJ lower bound is smaller than grid's origin.");
-            if (hi[a] > (n[a] - 1) * gap) throw std::runtime_error("ERROR: OBJ upper bound is out of the grid.");
-        }
-        int i0[3], i1[3];
-        for (int a = 0; a < 3; ++a) {
-            i0[a] = (int)(lo[a] / gap);
-            i1[a] = (int)(hi[a] / gap) + 1;
-        }
-        for (int ix = i0[0]; ix < i1[0]; ++ix)
-            for (int iy = i0[1]; iy < i1[1]; ++iy)
-                for (int iz = i0[2]; iz < i1[2]; ++iz)
-                    for (unsigned ip = 0; ip < ppc; ++ip) {
-                        const float wp[3] = {(float)(ix * gap + U(rng) * gap), (float)(iy * gap + U(rng) * gap),
-                                             (float)(iz * gap + U(rng) * gap)};
-                        // local = R^T ((world - T) / S)
-                        double q[3], l[3];
-                        for (int a = 0; a < 3; ++a) q[a] = (wp[a] - T[a]) / S[a];
-                        for (int a = 0; a < 3; ++a) l[a] = R.m[a] * q[0] + R.m[3 + a] * q[1] + R.m[6 + a] * q[2];
-                        bool in;
-                        if (shape == 0) in = std::fabs(l[0]) <= 0.5 && std::fabs(l[1]) <= 0.5 && std::fabs(l[2]) <= 0.5;
-                        else if (shape == 1) in = l[0] * l[0] + l[1] * l[1] + l[2] * l[2] <= 0.25;
-                        else if (shape == 2) in = l[0] * l[0] + l[2] * l[2] <= 0.25 && std::fabs(l[1]) <= 0.5;
-                        else in = mesh.inside(l);
-                        if (in) out.insert(out.end(), {wp[0], wp[1], wp[2]});
-                    }
+        int64_t cnt = 0;
+        check(mpm_seed(&so, 3, gap, nullptr, (int)ppc, seed, device, nullptr, 0, &cnt), nullptr);
+        out.resize((size_t)cnt * 3);
+        if (cnt > 0) check(mpm_seed(&so, 3, gap, nullptr, (int)ppc, seed, device, out.data(), out.size(), &cnt), nullptr);
     }
 };
 

@@ -51,6 +51,15 @@ class Options(C.Structure):
                 ("kernel_config", C.c_int), ("adaptive_dt", C.c_int), ("cfl", C.c_float)]
 
 
+SHAPE_CUBE, SHAPE_SPHERE, SHAPE_CYLINDER, SHAPE_MESH = 0, 1, 2, 3
+
+
+class SeedObject(C.Structure):
+    _fields_ = [("shape", C.c_int), ("rotation", C.c_double * 9), ("scale", C.c_double * 3),
+                ("translation", C.c_double * 3), ("vertices", _FP), ("n_vertices", C.c_int64),
+                ("triangles", C.POINTER(C.c_int32)), ("n_triangles", C.c_int64)]
+
+
 class SurrogateTrainOptions(C.Structure):
     _fields_ = [("n_samples", C.c_int64), ("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_float),
                 ("lr_final", C.c_float), ("sigma", C.c_float), ("rotation_fraction", C.c_float),
@@ -106,6 +115,8 @@ EXPORTS = {
     "mpm_surrogate_save": (C.c_int, [C.c_void_p, C.c_char_p]),
     "mpm_surrogate_load": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
     "mpm_set_stress_mode": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "mpm_seed": (C.c_int, [C.POINTER(SeedObject), C.c_int, C.c_double, C.POINTER(C.c_double), C.c_int, C.c_uint64,
+                           C.c_int, _FP, C.c_size_t, C.POINTER(C.c_int64)]),
     "mpm_get_stress_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
 }
 
