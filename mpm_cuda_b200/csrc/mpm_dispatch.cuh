@@ -11,8 +11,9 @@ namespace mpm {
 using FusedFn = void (*)(ParticleBuf, FusedArgs);
 using SurFn = void (*)(ParticleBuf, FusedArgs, SurArgs);
 
-// k_g2p2g<dim, mat, kFusedCfgs[ci]>
-FusedFn fused_fn(int dim, int mat, int ci);
+// k_g2p2g<dim, mat, kFusedCfgs[ci], fixed_scene>; fixed_scene: one scene whose
+// parameters do not change during the run, passed in FusedArgs::scene
+FusedFn fused_fn(int dim, int mat, int ci, bool fixed_scene);
 // k_g2p2g_sur<kFusedCfgs[ci]> (3D jello)
 SurFn sur_fn(int ci);
 

@@ -309,6 +309,9 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     if ((rc = alloc((void**)&groups_d, std::max<size_t>(1, groups_h.size()) * sizeof(GroupParams), "groups")) != MPM_OK)
         return rc;
     if ((rc = alloc((void**)&scenes_d, scenes_h.size() * sizeof(SceneParams), "scenes")) != MPM_OK) return rc;
+    // the device scene table never changes in such a run (only adaptive dt
+    // writes it), so the fused kernels may carry the scene in their parameters
+    fixed_scene = scenes_h.size() == 1 && !opt.adaptive_dt;
     const size_t grid_bytes = (size_t)total_blocks * 64 * sizeof(float4);
     if ((rc = alloc((void**)&grid_mom, grid_bytes, "grid_mom")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&grid_vel, grid_bytes, "grid_vel")) != MPM_OK) return rc;
@@ -415,7 +418,7 @@ void Engine::set_config(int ci) {
     cfg = ci;
     for (int mat = 0; mat < kMats; ++mat) {
         int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_fn(dim, mat, ci), kFusedCfgs[ci].chunk, 0) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_fn(dim, mat, ci, fixed_scene), kFusedCfgs[ci].chunk, 0) !=
             cudaSuccess) {
             cudaGetLastError();  // the query failed: fall back to one CTA per SM
             per_sm = 1;
@@ -727,6 +730,7 @@ FusedArgs Engine::fused_args(int mat, bool bump) {
     A.err_word = err_d;
     A.fallback = (unsigned*)(counters + CNT_FALLBACK);
     A.speed_max = opt.adaptive_dt ? speed_max : nullptr;
+    A.scene = scenes_h[0];
     return A;
 }
 
@@ -758,7 +762,7 @@ void Engine::enqueue_g2p2g(int parity) {
             sur_fn(cfg)<<<sur_ctas[mat], ch, sur_dyn_smem(ch), stream>>>(buf(parity), A, SA);
             note_launch("k_g2p2g_sur");
         } else {
-            fused_fn(dim, mat, cfg)<<<fused_ctas[mat], kFusedCfgs[cfg].chunk, 0, stream>>>(buf(parity), A);
+            fused_fn(dim, mat, cfg, fixed_scene)<<<fused_ctas[mat], kFusedCfgs[cfg].chunk, 0, stream>>>(buf(parity), A);
             note_launch("fused_fn");
         }
     }

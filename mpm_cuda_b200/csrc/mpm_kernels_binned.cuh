@@ -257,7 +257,18 @@ struct FusedArgs {
     unsigned* err_word;
     unsigned* fallback;  // count of particles that used global memory
     unsigned* speed_max; // adaptive dt: per scene max of |v| + wave (float bits); null when off
+    // the one scene of a single-scene run with a fixed dt, read by the kernels
+    // built with FIXED = true from their parameters (constant bank operands,
+    // no loads) instead of from `scenes`
+    SceneParams scene;
 };
+
+// the scene of chunk's scene index si: from the kernel parameters when FIXED
+template <bool FIXED>
+__device__ __forceinline__ const SceneParams& chunk_scene(const FusedArgs& A, int si) {
+    if constexpr (FIXED) return A.scene;
+    else return A.scenes[si];
+}
 
 template <int D>
 __device__ __forceinline__ int tv_idx(int x, int y, int z) {
@@ -465,7 +476,7 @@ struct SpeedFlush {
 // tv; every thread of the CTA calls it; post(scene index) runs after the
 // body's barrier.  Three barriers per chunk: window landed, body done (touched
 // complete, window free), loop state published.
-template <int D, int NT, class Body, class Post>
+template <int D, int NT, bool FIXED = false, class Body, class Post>
 __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][TileShape<D>::VN],
                                            unsigned (&touched)[2], int (&s_cn)[2], Body body, Post post) {
     const int nch = *A.n_chunks;
@@ -490,7 +501,7 @@ __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][T
         __syncthreads();     // everyone's
         const Chunk ch = A.chunks[cur];
         const int si = scene_of_block(A.scenes, A.n_scenes, ch.block);
-        const SceneParams& sc = A.scenes[si];
+        const SceneParams& sc = chunk_scene<FIXED>(A, si);
         int o[3];
         tile_origin<D>(sc, ch.block - sc.block_off, o);
         body(ch, sc, o, tv[b], &touched[b]);
@@ -513,8 +524,9 @@ __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][T
 // substep (MPMCUDA.cu:310-741 in one pass: the reference runs P2G, VelUpdate
 // and InterpolateAndMove as three kernels with full-grid sweeps and host
 // syncs between them).  The P2G scatter reduces straight to global memory
-// with float4 vector reductions (red.global.add.v4.f32).
-template <int D, int MAT, int CHUNK, int MINB>
+// with float4 vector reductions (red.global.add.v4.f32).  FIXED: the scene
+// comes from A.scene (one scene, dt fixed for the run).
+template <int D, int MAT, int CHUNK, int MINB, bool FIXED>
 __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs A) {
     using P = Planes<D>;
     using TS = TileShape<D>;
@@ -526,8 +538,8 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
     if (A.bump_epoch && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.epoch, 1);
     if (threadIdx.x == 0) s_speed = 0u;
     SpeedFlush speed;
-    chunk_loop<D, CHUNK>(A, tv, touched, s_cn,
-                         [&](const Chunk& ch, const SceneParams& sc, const int* o, const float4* w, unsigned* tb) {
+    chunk_loop<D, CHUNK, FIXED>(A, tv, touched, s_cn,
+                                [&](const Chunk& ch, const SceneParams& sc, const int* o, const float4* w, unsigned* tb) {
         unsigned speed_bits = 0u;
         if ((int)threadIdx.x < ch.count) {
             const long long i = (long long)ch.start + threadIdx.x;
