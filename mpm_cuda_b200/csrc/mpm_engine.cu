@@ -26,7 +26,16 @@ constexpr int kMaxGroups = 65535;
 constexpr int kDefaultRebinInterval = 16;
 // device counters: chunk list lengths and cursors per material, active
 // block count, grid epoch, tile fallbacks, re-binnings
-enum { CNT_CHUNKS = 0, CNT_ACTIVE = 3, CNT_EPOCH = 4, CNT_CURSOR = 5, CNT_FALLBACK = 8, CNT_REBINS = 9, CNT_N = 16 };
+enum {
+    CNT_CHUNKS = 0,
+    CNT_ACTIVE = 3,
+    CNT_EPOCH = 4,
+    CNT_CURSOR = 5,
+    CNT_FALLBACK = 8,
+    CNT_REBINS = 9,
+    CNT_UPDATE_DONE = 10,
+    CNT_N = 16
+};
 
 // out[id[i]] = in[i] for every plane (storage order -> creation order)
 __global__ void k_unpermute(const float* __restrict__ in, float* __restrict__ out, const uint32_t* __restrict__ id,
@@ -84,6 +93,11 @@ int Engine::cuda_fail(cudaError_t e, const char* what) {
 // records the first failing launch (by name) since the last take_launch_error()
 void Engine::note_launch(const char* what) {
     const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess && launch_error.empty()) launch_error = std::string(what) + ": " + cudaGetErrorString(e);
+}
+
+// the same for a launch whose status the launch call returned
+void Engine::note_launch_status(const char* what, cudaError_t e) {
     if (e != cudaSuccess && launch_error.empty()) launch_error = std::string(what) + ": " + cudaGetErrorString(e);
 }
 
@@ -734,20 +748,34 @@ FusedArgs Engine::fused_args(int mat, bool bump) {
     return A;
 }
 
+// launch attributes of a kernel that calls pdl_wait before it reads what the
+// kernel ahead of it wrote (programmatic dependent launch)
+static cudaLaunchConfig_t pdl_config(unsigned grid, unsigned block, size_t smem, cudaStream_t stream,
+                                     cudaLaunchAttribute* attr) {
+    cudaLaunchConfig_t c = {};
+    c.gridDim = dim3(grid);
+    c.blockDim = dim3(block);
+    c.dynamicSmemBytes = smem;
+    c.stream = stream;
+    attr->id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr->val.programmaticStreamSerializationAllowed = 1;
+    c.attrs = attr;
+    c.numAttrs = 1;
+    return c;
+}
+
 void Engine::enqueue_grid_update() {
     const int n_scenes = (int)scenes_h.size();
-    if (dim == 3)
-        k_grid_update_active<3><<<update_ctas, 256, 0, stream>>>(grid_mom, grid_vel, active, counters + CNT_ACTIVE,
-                                                                 blk_flag, blk_epoch, counters + CNT_EPOCH, scenes_d,
-                                                                 n_scenes);
-    else
-        k_grid_update_active<2><<<update_ctas, 256, 0, stream>>>(grid_mom, grid_vel, active, counters + CNT_ACTIVE,
-                                                                 blk_flag, blk_epoch, counters + CNT_EPOCH, scenes_d,
-                                                                 n_scenes);
-    note_launch("k_grid_update_active");
-    // the fused launches append the blocks of the next substep from zero
-    cudaMemsetAsync(counters + CNT_ACTIVE, 0, sizeof(int), stream);
-    cudaMemsetAsync(counters + CNT_CURSOR, 0, kMats * sizeof(int), stream);
+    // the kernel's last CTA zeroes the active-block count and the chunk
+    // cursors, so the fused launches append the next substep's blocks from zero
+    cudaLaunchAttribute attr;
+    const cudaLaunchConfig_t lc = pdl_config(update_ctas, 256, 0, stream, &attr);
+    auto k = dim == 3 ? k_grid_update_active<3> : k_grid_update_active<2>;
+    const cudaError_t e = cudaLaunchKernelEx(&lc, k, grid_mom, grid_vel, (const int*)active, counters + CNT_ACTIVE,
+                                             blk_flag, blk_epoch, (const int*)(counters + CNT_EPOCH),
+                                             (const SceneParams*)scenes_d, n_scenes, counters + CNT_CURSOR, (int)kMats,
+                                             (unsigned*)(counters + CNT_UPDATE_DONE));
+    note_launch_status("k_grid_update_active", e);
 }
 
 void Engine::enqueue_g2p2g(int parity) {
@@ -762,7 +790,10 @@ void Engine::enqueue_g2p2g(int parity) {
             sur_fn(cfg)<<<sur_ctas[mat], ch, sur_dyn_smem(ch), stream>>>(buf(parity), A, SA);
             note_launch("k_g2p2g_sur");
         } else {
-            fused_fn(dim, mat, cfg, fixed_scene)<<<fused_ctas[mat], kFusedCfgs[cfg].chunk, 0, stream>>>(buf(parity), A);
+            cudaLaunchAttribute attr;
+            const cudaLaunchConfig_t lc = pdl_config(fused_ctas[mat], kFusedCfgs[cfg].chunk, 0, stream, &attr);
+            const cudaError_t e = cudaLaunchKernelEx(&lc, fused_fn(dim, mat, cfg, fixed_scene), buf(parity), A);
+            note_launch_status("k_g2p2g", e);
             note_launch("fused_fn");
         }
     }

@@ -135,6 +135,7 @@ struct Engine {
    private:
     int cuda_fail(cudaError_t e, const char* what);
     void note_launch(const char* what);
+    void note_launch_status(const char* what, cudaError_t e);
     int take_launch_error();
     ParticleBuf buf(int p) const { return ParticleBuf{st[p], cap, gp[p], ids[p]}; }
     void enqueue_direct_substep();

@@ -212,12 +212,26 @@ __global__ void __launch_bounds__(128) k_p2g_prologue(ParticleBuf pb, long long 
 // Grid update of the active blocks: velocity into grid_vel, momentum buffer
 // cleared for the next P2G, block flag reset, block epoch stamped.
 // 64 threads per block, 4 blocks per CTA, persistent over the list.
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may start before the kernel ahead of it in the stream ends;
+// pdl_wait blocks until that kernel has completed and its writes are visible
+// (immediately when launched without the attribute), pdl_trigger lets the
+// next kernel in the stream begin launching.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+// Grid update of the blocks P2G touched.  The last CTA to finish resets the
+// active-block count and the fused kernels' chunk cursors for the next pass
+// (every CTA has read the count before it counts itself done).
 template <int D>
 __global__ void __launch_bounds__(256) k_grid_update_active(float4* __restrict__ grid_mom, float4* __restrict__ grid_vel,
-                                                            const int* __restrict__ active, const int* __restrict__ n_active,
+                                                            const int* __restrict__ active, int* __restrict__ n_active,
                                                             unsigned* __restrict__ blk_flag, int* __restrict__ blk_epoch,
                                                             const int* __restrict__ epoch,
-                                                            const SceneParams* __restrict__ scenes, int n_scenes) {
+                                                            const SceneParams* __restrict__ scenes, int n_scenes,
+                                                            int* __restrict__ cursors, int n_cursors,
+                                                            unsigned* __restrict__ done) {
+    pdl_wait();
     const int na = *n_active;
     const int ep = *epoch;
     const int lane = threadIdx.x & 63;
@@ -236,6 +250,13 @@ __global__ void __launch_bounds__(256) k_grid_update_active(float4* __restrict__
             blk_epoch[b] = ep;
         }
     }
+    __syncthreads();
+    if (threadIdx.x == 0 && atomicAdd(done, 1u) == gridDim.x - 1) {
+        *n_active = 0;
+        for (int k = 0; k < n_cursors; ++k) cursors[k] = 0;
+        *done = 0u;
+    }
+    pdl_trigger();
 }
 
 // ------------------------------------------------------------ G2P2G --
@@ -535,6 +556,8 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
     __shared__ int s_cn[2];
     __shared__ unsigned s_speed;                    // adaptive dt: this chunk's max signal speed
 
+    pdl_wait();     // the grid update ahead of this launch has finished
+    pdl_trigger();  // the next pass may launch; it waits for this one to end
     if (A.bump_epoch && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.epoch, 1);
     if (threadIdx.x == 0) s_speed = 0u;
     SpeedFlush speed;
