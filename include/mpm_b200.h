@@ -84,6 +84,7 @@ enum mpm_device_error {
     MPM_DEVERR_OUT_OF_GRID = 1, /* a particle's stencil left its grid */
     MPM_DEVERR_NONFINITE = 2,   /* NaN or Inf in particle state */
     MPM_DEVERR_DET = 4,         /* det F <= 0, det Fp <= 0 or J <= 0 */
+    MPM_DEVERR_BINNING = 8,     /* internal: particle binning counts disagreed */
     MPM_DEVERR_TIMEOUT = 16     /* a bounded device-side wait gave up */
 };
 

@@ -21,7 +21,7 @@ BC_STICKY, BC_SLIP, BC_SEPARATE = 0, 1, 2
 P2G_ATOMIC, P2G_DETERMINISTIC, P2G_DIRECT = 0, 1, 2
 STRESS_PLAIN, STRESS_SURROGATE = 0, 1
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_SIM, ERR_IO = 0, -1, -2, -3, -4, -5, -6
-DEVERR_OUT_OF_GRID, DEVERR_NONFINITE, DEVERR_DET, DEVERR_TIMEOUT = 1, 2, 4, 16
+DEVERR_OUT_OF_GRID, DEVERR_NONFINITE, DEVERR_DET, DEVERR_BINNING, DEVERR_TIMEOUT = 1, 2, 4, 8, 16
 
 _FP = C.POINTER(C.c_float)
 

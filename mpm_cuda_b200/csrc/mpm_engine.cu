@@ -334,7 +334,13 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
         if ((rc = alloc((void**)&keys[p], cap * sizeof(unsigned long long), "sort keys")) != MPM_OK) return rc;
         if ((rc = alloc((void**)&vals[p], cap * sizeof(unsigned), "sort values")) != MPM_OK) return rc;
     }
-    if ((rc = alloc((void**)&cell_count, total_blocks * 64 * sizeof(int), "cell counts")) != MPM_OK) return rc;
+    for (const GroupParams& g : groups_h) mat_present[g.type] = true;
+    mat_slots = MatSlots{};
+    for (int m = 0; m < kMats; ++m)
+        if (mat_present[m]) mat_slots.s[m] = mat_slots.n++;
+    mat_slots.n = std::max(mat_slots.n, 1);
+    const long long n_cell_counts = total_blocks * 64 * mat_slots.n;
+    if ((rc = alloc((void**)&cell_count, n_cell_counts * sizeof(int), "cell counts")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&cell_end, total_blocks * 64 * sizeof(int), "cell ends")) != MPM_OK) return rc;
     {
         const int src_planes = dim == 3 ? SrcPlanes<3>::COUNT : SrcPlanes<2>::COUNT;
@@ -351,28 +357,12 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     if ((rc = alloc((void**)&scene_time, scenes_h.size() * sizeof(double), "scene times")) != MPM_OK) return rc;
     list_cap = cap / kFusedCfgs[kNumFusedCfgs - 1].chunk + std::min<long long>(cap, total_blocks) + 1;
     if ((rc = alloc((void**)&chunks, kMats * list_cap * sizeof(Chunk), "chunks")) != MPM_OK) return rc;
-    key_bits = 12;
-    while (key_bits < 64 && (1LL << (key_bits - 12)) < total_blocks) ++key_bits;
     det_key_bits = 1;
     while (det_key_bits < 64 && (1LL << det_key_bits) <= total_blocks * 64) ++det_key_bits;
-    // binning keys are sorted as 32-bit words when they fit (fewer bytes per
-    // radix pass); the key buffers are allocated as 64-bit either way
-    if (key_bits <= 32) {
-        cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp_bytes, keys32(0), keys32(1), vals[0], vals[1], (int)cap, 0,
-                                        key_bits);
-    } else {
-        cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp_bytes, keys[0], keys[1], vals[0], vals[1], (int)cap, 0,
-                                        key_bits);
-    }
-    {
-        size_t det_bytes = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, det_bytes, keys[0], keys[1], vals[0], vals[1], (int)cap, 0, 64);
-        sort_tmp_bytes = std::max(sort_tmp_bytes, det_bytes);
-    }
+    cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp_bytes, keys[0], keys[1], vals[0], vals[1], (int)cap, 0, 64);
     if ((rc = alloc(&sort_tmp, sort_tmp_bytes, "sort temp")) != MPM_OK) return rc;
     cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp_bytes, seg_count, seg_start, (int)(total_blocks * 4));
     if ((rc = alloc(&scan_tmp, scan_tmp_bytes, "scan temp")) != MPM_OK) return rc;
-    for (const GroupParams& g : groups_h) mat_present[g.type] = true;
     if ((rc = alloc((void**)&pos_out, cap * D * sizeof(float), "positions")) != MPM_OK) return rc;
 
     e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
@@ -391,7 +381,7 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     if (e == cudaSuccess) e = cudaMemset(grid_vel, 0, grid_bytes);
     if (e == cudaSuccess) e = cudaMemset(err_d, 0, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(blk_flag, 0, total_blocks * sizeof(unsigned));
-    if (e == cudaSuccess) e = cudaMemset(cell_count, 0, total_blocks * 64 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(cell_count, 0, n_cell_counts * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(cell_end, 0, total_blocks * 64 * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(seg_count, 0, total_blocks * 4 * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(blk_epoch, 0xff, total_blocks * sizeof(int));
@@ -668,59 +658,42 @@ void Engine::enqueue_direct_substep() {
     }
 }
 
-// radix sort of the particles of buffer `from` by (home block, material,
-// rank in cell, cell) into the other buffer, and the chunk lists of the result
+// bins the particles of buffer `from` by (home block, material) into the
+// other buffer, rank-major within each segment (counting placement, no sort),
+// and builds the chunk lists of the result
 void Engine::enqueue_rebin(int from) {
     const int to = 1 - from;
     const long long n_segs = total_blocks * 4;
+    int* rank = reinterpret_cast<int*>(vals[0]);
     cudaMemsetAsync(counters + CNT_CHUNKS, 0, kMats * sizeof(int), stream);
+    const unsigned nb = grid_blocks(n_particles, 256);
     if (n_particles > 0) {
-        const unsigned nb = grid_blocks(n_particles, 256);
-        if (key_bits <= 32) {
-            if (dim == 3)
-                k_bin_key<3, unsigned><<<nb, 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d, keys32(0),
-                                                               vals[0], cell_count, seg_count);
-            else
-                k_bin_key<2, unsigned><<<nb, 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d, keys32(0),
-                                                               vals[0], cell_count, seg_count);
-            note_launch("k_bin_key");
-            cub::DeviceRadixSort::SortPairs(sort_tmp, sort_tmp_bytes, keys32(0), keys32(1), vals[0], vals[1],
-                                            (int)n_particles, 0, key_bits, stream);
-        } else {
-            if (dim == 3)
-                k_bin_key<3, unsigned long long><<<nb, 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d,
-                                                                         keys[0], vals[0], cell_count, seg_count);
-            else
-                k_bin_key<2, unsigned long long><<<nb, 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d,
-                                                                         keys[0], vals[0], cell_count, seg_count);
-            note_launch("k_bin_key");
-            cub::DeviceRadixSort::SortPairs(sort_tmp, sort_tmp_bytes, keys[0], keys[1], vals[0], vals[1],
-                                            (int)n_particles, 0, key_bits, stream);
-        }
-        note_launch("cub::DeviceRadixSort::SortPairs");
         if (dim == 3)
-            k_bin_gather<3><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), buf(to), n_particles,
-                                                                               vals[1]);
+            k_bin_count<3><<<nb, 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d, mat_slots, keys[0], rank,
+                                                   cell_count, seg_count);
         else
-            k_bin_gather<2><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(from), buf(to), n_particles,
-                                                                               vals[1]);
-        note_launch("k_bin_gather");
+            k_bin_count<2><<<nb, 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d, mat_slots, keys[0], rank,
+                                                   cell_count, seg_count);
+        note_launch("k_bin_count");
     }
     cub::DeviceScan::ExclusiveSum(scan_tmp, scan_tmp_bytes, seg_count, seg_start, (int)n_segs, stream);
     note_launch("cub::DeviceScan::ExclusiveSum");
+    if (n_particles > 0) {
+        if (dim == 3)
+            k_bin_place<3><<<nb, 256, 0, stream>>>(buf(from), buf(to), n_particles, keys[0], rank, cell_count,
+                                                   seg_count, seg_start, mat_slots, err_d);
+        else
+            k_bin_place<2><<<nb, 256, 0, stream>>>(buf(from), buf(to), n_particles, keys[0], rank, cell_count,
+                                                   seg_count, seg_start, mat_slots, err_d);
+        note_launch("k_bin_place");
+    }
     k_make_chunks<<<grid_blocks(n_segs, 256), 256, 0, stream>>>(seg_count, seg_start, n_segs, chunks, list_cap,
                                                                 counters + CNT_CHUNKS, kFusedCfgs[cfg].chunk);
     note_launch("k_make_chunks");
-    if (n_particles > 0)
-    {
-        if (key_bits <= 32)
-            k_bin_reset<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys32(1), n_particles, cell_count,
-                                                                           seg_count);
-        else
-            k_bin_reset<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys[1], n_particles, cell_count,
-                                                                           seg_count);
+    if (n_particles > 0) {
+        k_bin_reset<<<nb, 256, 0, stream>>>(keys[0], n_particles, mat_slots, cell_count, seg_count);
+        note_launch("k_bin_reset");
     }
-    note_launch("k_bin_reset");
     k_count_rebin<<<1, 1, 0, stream>>>(counters + CNT_REBINS);
     note_launch("k_count_rebin");
     sorted_order = true;

@@ -46,11 +46,14 @@ struct Engine {
     unsigned* err_d = nullptr;
 
     // binning and block activity
-    unsigned long long* keys[2] = {nullptr, nullptr};  // radix sort keys in / out
-    // the same buffers as 32-bit keys (binning keys of at most 32 bits)
-    unsigned* keys32(int p) const { return reinterpret_cast<unsigned*>(keys[p]); }
-    unsigned* vals[2] = {nullptr, nullptr};            // particle index in / sorted
-    int* cell_count = nullptr;  // per node of every block: particles whose base is that node
+    // binning: keys[0] = (home block, material, cell) and vals[0] = rank in
+    // the cell of each particle; the deterministic mode sorts keys / vals
+    unsigned long long* keys[2] = {nullptr, nullptr};
+    unsigned* vals[2] = {nullptr, nullptr};
+    // binning: per (block, present material) 64 cell counts; the
+    // deterministic mode: per base node of every block
+    int* cell_count = nullptr;
+    MatSlots mat_slots{};       // compact index of each present material
     int* cell_end = nullptr;    // deterministic mode: end of each base node's records
     float* det_src = nullptr;   // deterministic mode: P2G source records
     int det_key_bits = 64;
@@ -61,7 +64,6 @@ struct Engine {
     size_t sort_tmp_bytes = 0;
     void* scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
-    int key_bits = 64;
     Chunk* chunks = nullptr;    // kMats lists of list_cap entries
     long long list_cap = 0;
     bool mat_present[3] = {false, false, false};

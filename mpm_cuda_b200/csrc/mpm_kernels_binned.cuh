@@ -24,9 +24,7 @@
 namespace mpm {
 
 constexpr int kMaxChunk = 256;  // largest chunk (particles per fused CTA)
-constexpr int kMaxRank = 15;    // rank-in-cell field of the sort key (4 bits)
 constexpr int kMats = 3;        // JELLO, SNOW, WATER
-
 
 struct Chunk {
     int block;  // global block index (scene block_off + local block)
@@ -76,12 +74,18 @@ __device__ __forceinline__ void home_of(const SceneParams& sc, const float* x, l
     cell = c[0] + BlockShape<D>::SIDE * (c[1] + BlockShape<D>::SIDE * c[2]);  // 0..63
 }
 
-// sort key (block, material, rank in cell, cell) and the identity payload
-template <int D, class K>
-__global__ void __launch_bounds__(256) k_bin_key(ParticleBuf pb, long long n, const GroupParams* __restrict__ groups,
-                                                 const SceneParams* __restrict__ scenes, K* __restrict__ keys,
-                                                 unsigned* __restrict__ vals, int* __restrict__ cell_count,
-                                                 int* __restrict__ seg_count) {
+// Binning by counting, without a sort.  The particles of each (home block,
+// material) segment are ordered rank-major: first every cell's rank-0
+// particle (cells ascending), then every rank-1 particle, and so on, so the
+// lanes of a warp sit in distinct cells.
+
+// Pass 1: home block b, cell c and material m of every particle, its rank
+// among the particles of (b, m, c) and the size of segment (b, m).
+template <int D>
+__global__ void __launch_bounds__(256) k_bin_count(ParticleBuf pb, long long n, const GroupParams* __restrict__ groups,
+                                                   const SceneParams* __restrict__ scenes, MatSlots ms,
+                                                   unsigned long long* __restrict__ key, int* __restrict__ rank,
+                                                   int* __restrict__ cell_count, int* __restrict__ seg_count) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float x[D];
@@ -92,21 +96,50 @@ __global__ void __launch_bounds__(256) k_bin_key(ParticleBuf pb, long long n, co
     long long b;
     int c;
     home_of<D>(sc, x, b, c);
-    const int r = min(atomicAdd(&cell_count[b * 64 + c], 1), kMaxRank);
+    rank[i] = atomicAdd(&cell_count[(b * ms.n + ms.s[g.type]) * 64 + c], 1);
     atomicAdd(&seg_count[b * 4 + g.type], 1);
-    // K is 32-bit when the block index fits in 20 bits
-    keys[i] = (K)(((unsigned long long)b << 12) | ((unsigned long long)g.type << 10) | ((unsigned long long)r << 6) |
-                  (unsigned long long)c);
-    vals[i] = (unsigned)i;
+    key[i] = ((unsigned long long)b << 8) | ((unsigned long long)g.type << 6) | (unsigned long long)c;
 }
 
-// dst[j] = src[perm[j]] for every plane, group and creation index
+// Pass 2 (after the scan of the segment sizes): the slot of particle (r, c)
+// in its segment is
+//   sum over cells c' of min(n_c', r)   (particles of lower rank)
+// + #{c' < c : n_c' > r}                (rank r in lower cells),
+// n_c' the segment's cell counts; the particle's state moves there.  Ranks
+// are exact, so the slots are a permutation of the segment; a slot outside
+// it (inconsistent counts) is reported, not written.
 template <int D>
-__global__ void __launch_bounds__(256) k_bin_gather(ParticleBuf src, ParticleBuf dst, long long n,
-                                                    const unsigned* __restrict__ perm) {
-    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    const long long i = perm[j];
+__global__ void __launch_bounds__(256) k_bin_place(ParticleBuf src, ParticleBuf dst, long long n,
+                                                   const unsigned long long* __restrict__ key,
+                                                   const int* __restrict__ rank, const int* __restrict__ cell_count,
+                                                   const int* __restrict__ seg_count,
+                                                   const int* __restrict__ seg_start, MatSlots ms,
+                                                   unsigned* __restrict__ err) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned long long k = key[i];
+    const long long b = (long long)(k >> 8);
+    const int m = (int)((k >> 6) & 3), c = (int)(k & 63);
+    const int r = rank[i];
+    const int4* cnt = reinterpret_cast<const int4*>(cell_count + (b * ms.n + ms.s[m]) * 64);
+    int lower = 0, before = 0;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const int4 v = cnt[q];
+        const int nc[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            lower += min(nc[t], r);
+            before += (4 * q + t < c && nc[t] > r) ? 1 : 0;
+        }
+    }
+    const int off = lower + before;
+    const int seg = (int)(b * 4 + m);
+    if (off < 0 || off >= seg_count[seg]) {
+        atomicOr(err, ERR_BINNING);
+        return;
+    }
+    const long long j = (long long)seg_start[seg] + off;
 #pragma unroll
     for (int p = 0; p < Planes<D>::COUNT; ++p) dst.s[p * dst.cap + j] = src.s[p * src.cap + i];
     dst.grp[j] = src.grp[i];
@@ -136,16 +169,17 @@ static __global__ void __launch_bounds__(256) k_make_chunks(const int* __restric
     }
 }
 
-// zero the cell and segment counters the last k_bin_key touched
-template <class K>
-__global__ void __launch_bounds__(256) k_bin_reset(const K* __restrict__ keys, long long n,
-                                                   int* __restrict__ cell_count, int* __restrict__ seg_count) {
-    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    const unsigned long long k = keys[j];
-    const long long b = (long long)(k >> 12);
-    cell_count[b * 64 + (int)(k & 63)] = 0;
-    seg_count[b * 4 + (int)((k >> 10) & 3)] = 0;
+// zero the cell and segment counters that k_bin_count touched
+static __global__ void __launch_bounds__(256) k_bin_reset(const unsigned long long* __restrict__ key, long long n,
+                                                          MatSlots ms, int* __restrict__ cell_count,
+                                                          int* __restrict__ seg_count) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned long long k = key[i];
+    const long long b = (long long)(k >> 8);
+    const int m = (int)((k >> 6) & 3);
+    cell_count[(b * ms.n + ms.s[m]) * 64 + (int)(k & 63)] = 0;
+    seg_count[b * 4 + m] = 0;
 }
 
 static __global__ void k_count_rebin(int* counter) { *counter += 1; }

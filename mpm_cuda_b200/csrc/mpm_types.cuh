@@ -9,7 +9,7 @@ namespace mpm {
 // material type values match the reference enum (Elasiticity.cuh:10-11)
 enum : int { JELLO = 0, SNOW = 1, WATER = 2, SAND = 3 };
 enum : int { BC_STICKY = 0, BC_SLIP = 1, BC_SEPARATE = 2 };
-enum : unsigned { ERR_OUT_OF_GRID = 1u, ERR_NONFINITE = 2u, ERR_DET = 4u, ERR_TIMEOUT = 16u };
+enum : unsigned { ERR_OUT_OF_GRID = 1u, ERR_NONFINITE = 2u, ERR_DET = 4u, ERR_BINNING = 8u, ERR_TIMEOUT = 16u };
 
 // One particle group: material + per-particle mass/volume (ParticleGroup,
 // MPMSimulator.cuh:30-52; Material, Elasiticity.cuh:19-45).
@@ -45,6 +45,13 @@ struct SceneParams {
     // adaptive dt (MPM_P2G_ATOMIC): dt_next = clamp(cfl h / max(|v| + wave), dt_min, dt_max)
     float dt_max, dt_min, cfl;
     int adaptive;
+};
+
+// Compact index of each present material in the binning's per-cell
+// counters, which hold n slots of 64 cells per block.
+struct MatSlots {
+    int s[4];
+    int n;
 };
 
 // Particle state: component planes of one FP32 buffer, plane stride `cap`.
