@@ -628,6 +628,10 @@ void Engine::drop_graphs() {
             if (g) cudaGraphExecDestroy(g);
             g = nullptr;
         }
+    for (auto& g : run_graphs) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
 }
 
 // ---------------------------------------------------------- launches --
@@ -887,14 +891,15 @@ int Engine::prologue() {
     return MPM_OK;
 }
 
-int Engine::build_graph(int parity, int rebin) {
+// captures a re-binning and one substep (rebin), or `count` plain substeps
+int Engine::build_graph(int parity, int rebin, int count, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
     MPM_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "graph capture begin");
     if (rebin) {
         enqueue_rebin(parity);
         enqueue_fused_substep(1 - parity);
     } else {
-        enqueue_fused_substep(parity);
+        for (int k = 0; k < count; ++k) enqueue_fused_substep(parity);
     }
     cudaError_t e = cudaStreamEndCapture(stream, &g);
     if (e != cudaSuccess) {
@@ -906,10 +911,10 @@ int Engine::build_graph(int parity, int rebin) {
         cudaGraphDestroy(g);
         return MPM_ERR_CUDA;
     }
-    e = cudaGraphInstantiate(&graphs[parity][rebin], g, 0);
+    e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
-        graphs[parity][rebin] = nullptr;
+        *out = nullptr;
         return cuda_fail(e, "graph instantiate");
     }
     return MPM_OK;
@@ -978,11 +983,23 @@ int Engine::step(int n) {
             int rc = prologue();
             if (rc != MPM_OK) return rc;
         }
+        const int run = opt.rebin_interval - 1;  // plain substeps between two re-binnings
         for (int i = 0; i < n; ++i) {
             const int rebin = steps_since_rebin >= opt.rebin_interval ? 1 : 0;
+            if (opt.use_graph && !rebin && run > 1 && steps_since_rebin == 1 && n - i >= run) {
+                // the whole stretch up to the next re-binning as one graph
+                if (!run_graphs[cur]) {
+                    int rc = build_graph(cur, 0, run, &run_graphs[cur]);
+                    if (rc != MPM_OK) return rc;
+                }
+                MPM_CUDA_TRY(cudaGraphLaunch(run_graphs[cur], stream), "graph launch");
+                steps_since_rebin += run;
+                i += run - 1;
+                continue;
+            }
             if (opt.use_graph) {
                 if (!graphs[cur][rebin]) {
-                    int rc = build_graph(cur, rebin);
+                    int rc = build_graph(cur, rebin, 1, &graphs[cur][rebin]);
                     if (rc != MPM_OK) return rc;
                 }
                 MPM_CUDA_TRY(cudaGraphLaunch(graphs[cur][rebin], stream), "graph launch");

@@ -103,6 +103,8 @@ struct Engine {
 
     // substep graphs: [parity][rebin first]
     cudaGraphExec_t graphs[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    // per parity: the rebin_interval - 1 plain substeps between two re-binnings
+    cudaGraphExec_t run_graphs[2] = {nullptr, nullptr};
     bool grid_dirty = true;  // grid_mom does not hold the P2G of the current state
 
     double current_time = 0.0;
@@ -148,7 +150,7 @@ struct Engine {
     void enqueue_g2p2g(int parity);
     FusedArgs fused_args(int mat, bool bump);
     int prologue();
-    int build_graph(int parity, int rebin);
+    int build_graph(int parity, int rebin, int count, cudaGraphExec_t* out);
     void drop_graphs();
     int unpermute_to_alt();
     bool fused() const { return opt.p2g_mode == MPM_P2G_ATOMIC; }
