@@ -529,8 +529,10 @@ struct SpeedFlush {
 // processed, so the cursor atomic and the window's L2 round trips are off the
 // critical path.  body(ch, sc, o, tv, touched) runs with chunk ch's window in
 // tv; every thread of the CTA calls it; post(scene index) runs after the
-// body's barrier.  Three barriers per chunk: window landed, body done (touched
-// complete, window free), loop state published.
+// body's barrier.  Two barriers per chunk: (1) window landed, the chunk after
+// next and the cleared touched word published; (2) body done (touched
+// complete, window free).  Shared words of parity b = k & 1 are rewritten two
+// chunks later, after both barriers of the chunk in between.
 template <int D, int NT, bool FIXED = false, class Body, class Post>
 __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][TileShape<D>::VN],
                                            unsigned (&touched)[2], int (&s_cn)[2], Body body, Post post) {
@@ -541,35 +543,30 @@ __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][T
     }
     __syncthreads();
     int cur = s_cn[0], nxt = s_cn[1];
+    __syncthreads();  // s_cn is rewritten below
     if (cur < nch) prefetch_velocity_tile<D, NT>(A, cur, tv[0]);
     cp_async_commit();
     for (int k = 0; cur < nch; ++k) {
         const int b = k & 1;
         if (nxt < nch) prefetch_velocity_tile<D, NT>(A, nxt, tv[b ^ 1]);
         cp_async_commit();
-        int after = 0;
         if (threadIdx.x == 0) {
-            after = atomicAdd(A.cursor, 1);
+            s_cn[b] = atomicAdd(A.cursor, 1);  // the chunk after next
             touched[b] = 0u;
         }
         cp_async_wait<1>();  // this thread's copies of the current window
-        __syncthreads();     // everyone's
+        __syncthreads();     // (1) everyone's; s_cn[b] and touched[b] published
         const Chunk ch = A.chunks[cur];
         const int si = scene_of_block(A.scenes, A.n_scenes, ch.block);
         const SceneParams& sc = chunk_scene<FIXED>(A, si);
         int o[3];
         tile_origin<D>(sc, ch.block - sc.block_off, o);
         body(ch, sc, o, tv[b], &touched[b]);
-        __syncthreads();
+        __syncthreads();     // (2)
         mark_touched<D>(touched[b], sc, o, A);
         post(si);
-        if (threadIdx.x == 0) {
-            s_cn[0] = nxt;
-            s_cn[1] = after;
-        }
-        __syncthreads();
-        cur = s_cn[0];
-        nxt = s_cn[1];
+        cur = nxt;
+        nxt = s_cn[b];
     }
     cp_async_wait<0>();
 }
