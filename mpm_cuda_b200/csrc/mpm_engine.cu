@@ -691,8 +691,14 @@ void Engine::enqueue_rebin(int from) {
                                                    seg_count, seg_start, mat_slots, err_d);
         note_launch("k_bin_place");
     }
-    k_make_chunks<<<grid_blocks(n_segs, 256), 256, 0, stream>>>(seg_count, seg_start, n_segs, chunks, list_cap,
-                                                                counters + CNT_CHUNKS, kFusedCfgs[cfg].chunk);
+    if (dim == 3)
+        k_make_chunks<3><<<grid_blocks(n_segs, 256), 256, 0, stream>>>(seg_count, seg_start, n_segs, chunks, list_cap,
+                                                                       counters + CNT_CHUNKS, kFusedCfgs[cfg].chunk,
+                                                                       scenes_d, (int)scenes_h.size());
+    else
+        k_make_chunks<2><<<grid_blocks(n_segs, 256), 256, 0, stream>>>(seg_count, seg_start, n_segs, chunks, list_cap,
+                                                                       counters + CNT_CHUNKS, kFusedCfgs[cfg].chunk,
+                                                                       scenes_d, (int)scenes_h.size());
     note_launch("k_make_chunks");
     if (n_particles > 0) {
         k_bin_reset<<<nb, 256, 0, stream>>>(keys[0], n_particles, mat_slots, cell_count, seg_count);

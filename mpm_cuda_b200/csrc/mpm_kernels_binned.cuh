@@ -31,6 +31,8 @@ struct Chunk {
     int start;  // first sorted particle
     int count;  // particles in this chunk
     int mat;    // material of every particle of the chunk
+    int scene;  // scene of the block
+    int o[3];   // window origin: the home block's first node minus one per axis
 };
 
 // Tile layout.  3D: window 8^3; the velocity tile (float4) has strides
@@ -146,26 +148,41 @@ __global__ void __launch_bounds__(256) k_bin_place(ParticleBuf src, ParticleBuf 
     dst.id[j] = src.id[i];
 }
 
+// window origin of a chunk's home block: one node below the block
+template <int D>
+__device__ __forceinline__ void tile_origin(const SceneParams& sc, long long lb, int* o) {
+    constexpr int SIDE = TileShape<D>::SIDE;
+    o[0] = (int)(lb % sc.nb[0]) * SIDE - 1;
+    o[1] = (int)((lb / sc.nb[0]) % sc.nb[1]) * SIDE - 1;
+    o[2] = (D == 3) ? (int)(lb / ((long long)sc.nb[0] * sc.nb[1])) * SIDE - 1 : 0;
+}
+
 // one chunk per `chunk` particles of every non-empty (block, material)
-// segment, appended to that material's list
-static __global__ void __launch_bounds__(256) k_make_chunks(const int* __restrict__ seg_count,
+// segment, appended to that material's list, with its scene and window
+// origin (the block's coordinates, divided out once here)
+template <int D>
+__global__ void __launch_bounds__(256) k_make_chunks(const int* __restrict__ seg_count,
                                                      const int* __restrict__ seg_start, long long n_segs,
                                                      Chunk* __restrict__ chunks, long long list_cap,
-                                                     int* __restrict__ n_chunks, int chunk) {
+                                                     int* __restrict__ n_chunks, int chunk,
+                                                     const SceneParams* __restrict__ scenes, int n_scenes) {
     const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_segs) return;
     const int c = seg_count[s];
     if (c == 0) return;
     const int mat = (int)(s & 3);
     const int nch = (c + chunk - 1) / chunk;
-    const int o = atomicAdd(&n_chunks[mat], nch);
+    const int at = atomicAdd(&n_chunks[mat], nch);
+    Chunk ch;
+    ch.block = (int)(s >> 2);
+    ch.mat = mat;
+    ch.scene = scene_of_block(scenes, n_scenes, ch.block);
+    const SceneParams& sc = scenes[ch.scene];
+    tile_origin<D>(sc, ch.block - sc.block_off, ch.o);
     for (int j = 0; j < nch; ++j) {
-        Chunk ch;
-        ch.block = (int)(s >> 2);
         ch.start = seg_start[s] + j * chunk;
         ch.count = min(chunk, c - j * chunk);
-        ch.mat = mat;
-        chunks[mat * list_cap + o + j] = ch;
+        chunks[mat * list_cap + at + j] = ch;
     }
 }
 
@@ -332,14 +349,6 @@ __device__ __forceinline__ int tv_idx(int x, int y, int z) {
 
 // ---- pieces of the fused pass (shared by the plain and surrogate kernels)
 
-// window origin of a chunk's home block: one node below the block
-template <int D>
-__device__ __forceinline__ void tile_origin(const SceneParams& sc, long long lb, int* o) {
-    constexpr int SIDE = TileShape<D>::SIDE;
-    o[0] = (int)(lb % sc.nb[0]) * SIDE - 1;
-    o[1] = (int)((lb / sc.nb[0]) % sc.nb[1]) * SIDE - 1;
-    o[2] = (D == 3) ? (int)(lb / ((long long)sc.nb[0] * sc.nb[1])) * SIDE - 1 : 0;
-}
 
 // 16-byte asynchronous global -> shared copy (cp.async.cg), zero-filled
 // when `valid` is false (source size 0: nothing is read)
@@ -359,16 +368,24 @@ __device__ __forceinline__ void cp_async_wait() {
 template <int D, int NT>
 __device__ __forceinline__ void prefetch_velocity_tile(const FusedArgs& A, int c, float4* tv) {
     constexpr int T = TileShape<D>::T;
+    constexpr int S = BlockShape<D>::SHIFT;
+    constexpr int M = BlockShape<D>::SIDE - 1;
+    constexpr int SIDE = BlockShape<D>::SIDE;
     const Chunk ch = A.chunks[c];
-    const SceneParams& sc = A.scenes[scene_of_block(A.scenes, A.n_scenes, ch.block)];
-    int o[3];
-    tile_origin<D>(sc, ch.block - sc.block_off, o);
+    const SceneParams& sc = A.scenes[ch.scene];
+    const float4* g = A.grid_vel + sc.node_off;
     for (int t = threadIdx.x; t < TileShape<D>::N; t += NT) {
         const int tx = t % T, ty = (t / T) % T, tz = (D == 3) ? t / (T * T) : 0;
-        const int ix = o[0] + tx, iy = o[1] + ty, iz = o[2] + tz;
+        const int ix = ch.o[0] + tx, iy = ch.o[1] + ty, iz = ch.o[2] + tz;
         bool in = ix >= 0 && iy >= 0 && ix < sc.n[0] && iy < sc.n[1];
         if (D == 3) in = in && iz >= 0 && iz < sc.n[2];
-        const float4* src = in ? A.grid_vel + node_index<D>(sc, ix, iy, iz) : A.grid_vel;
+        const float4* src = A.grid_vel;  // not read when outside the grid
+        if (in) {
+            // blocked node index relative to the scene (< 2^31 nodes), as in node_index
+            int idx = (ix >> S) * 64 + (ix & M) + ((iy >> S) * sc.nb[0] * 64 + (iy & M) * SIDE);
+            if (D == 3) idx += (iz >> S) * sc.nb[0] * sc.nb[1] * 64 + (iz & M) * SIDE * SIDE;
+            src = g + idx;
+        }
         cp_async16(&tv[tv_idx<D>(tx, ty, tz)], src, in);
     }
 }
@@ -557,10 +574,9 @@ __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][T
         cp_async_wait<1>();  // this thread's copies of the current window
         __syncthreads();     // (1) everyone's; s_cn[b] and touched[b] published
         const Chunk ch = A.chunks[cur];
-        const int si = scene_of_block(A.scenes, A.n_scenes, ch.block);
+        const int si = ch.scene;
         const SceneParams& sc = chunk_scene<FIXED>(A, si);
-        int o[3];
-        tile_origin<D>(sc, ch.block - sc.block_off, o);
+        const int o[3] = {ch.o[0], ch.o[1], ch.o[2]};
         body(ch, sc, o, tv[b], &touched[b]);
         __syncthreads();     // (2)
         mark_touched<D>(touched[b], sc, o, A);
