@@ -62,6 +62,7 @@ __global__ void k_canonicalize(const float* __restrict__ in, float* __restrict__
 // out[i] = in[id[i]] for particles whose creation index lies in [lo, hi)
 __global__ void k_permute_range(const float* __restrict__ in, float* __restrict__ out, const uint32_t* __restrict__ id,
                                 long long n, long long cap, int planes, long long lo, long long hi) {
+    pdl_wait();  // launched early behind the fused pass: wait for its positions
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const long long j = id[i];
@@ -72,6 +73,7 @@ __global__ void k_permute_range(const float* __restrict__ in, float* __restrict_
 // positions of creation indices [lo, hi) as interleaved x[(id - lo) * dim + a]
 __global__ void k_gather_positions(const float* __restrict__ s, const uint32_t* __restrict__ id, long long n,
                                    long long cap, int dim, long long lo, long long hi, float* __restrict__ out) {
+    pdl_wait();  // launched early behind the fused pass: wait for its positions
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const long long j = id[i];
@@ -1105,9 +1107,11 @@ int Engine::get_positions_async(int scene, float* out, long long* ticket) {
     // scene < 0: every scene, concatenated in creation order
     const long long b = scene < 0 ? 0 : scene_begin[scene], n = scene < 0 ? n_particles : scene_count[scene];
     if (n > 0) {
-        k_gather_positions<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(st[cur], ids[cur], n_particles, cap, dim,
-                                                                              b, b + n, sl.dev);
-        MPM_CUDA_TRY(cudaGetLastError(), "gather launch");
+        cudaLaunchAttribute attr;
+        const cudaLaunchConfig_t lc = pdl_config(grid_blocks(n_particles, 256), 256, 0, stream, &attr);
+        MPM_CUDA_TRY(cudaLaunchKernelEx(&lc, k_gather_positions, (const float*)st[cur], (const uint32_t*)ids[cur],
+                                        n_particles, cap, dim, b, b + n, sl.dev),
+                     "gather launch");
     }
     MPM_CUDA_TRY(cudaEventRecord(sl.gathered, stream), "event record");
     MPM_CUDA_TRY(cudaStreamWaitEvent(copy_stream, sl.gathered, 0), "copy wait");
