@@ -43,8 +43,11 @@ UNIT = "particle-substeps/s"
 L2_FLUSH_BYTES = 256 << 20
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # plain-run substeps at which the surrogate's training set is harvested:
-# start, interval, snapshots, held-out offset after the last
+# start, interval, snapshots, held-out offset after the last.  The batched
+# scenes are harvested within their stated 500 substeps: past ~1,500 substeps
+# at the fixed dt = 1e-4, hardening makes some snow scenes break the CFL bound.
 SURROGATE_HARVEST = (1400, 200, 8, 350)
+SURROGATE_HARVEST_BY_WORKLOAD = {"c4": (100, 50, 6, 100)}
 
 
 def hbm_peak():
@@ -212,9 +215,12 @@ def surrogate_leg(args, sim, scenes, stream, flush, plain_ms_per_step: float):
         return {"unavailable": "no 3D jello group in this workload (snow's exact stress reuses the "
                                "decomposition of its plasticity clamp, so it keeps the plain path)"}
     fresh, _ = build_workload(args.workload, 0, 1)
+    hv = SURROGATE_HARVEST_BY_WORKLOAD.get(args.workload, SURROGATE_HARVEST)
     t0 = time.perf_counter()
-    train_F, held_F = harvest(fresh, start=SURROGATE_HARVEST[0], every=SURROGATE_HARVEST[1],
-                              count=SURROGATE_HARVEST[2], held=SURROGATE_HARVEST[3])
+    try:
+        train_F, held_F = harvest(fresh, start=hv[0], every=hv[1], count=hv[2], held=hv[3])
+    except L.MPMError as e:
+        return {"unavailable": f"the plain run that harvests the training set failed: {e}"}
     rng = np.random.default_rng(0)
     if train_F.shape[0] > 2_000_000:
         train_F = train_F[rng.choice(train_F.shape[0], 2_000_000, replace=False)]
@@ -225,13 +231,23 @@ def surrogate_leg(args, sim, scenes, stream, flush, plain_ms_per_step: float):
     loss = sur.train(train_F)
     t2 = time.perf_counter()
     err, accepted = stress_error(sur, held_F, solids[0].material.nu)
-    sim.set_stress_mode(L.STRESS_SURROGATE, sur)
-    sim.step(args.warmup)
-    sim.synchronize()
-    t_ms = time_substeps(sim, stream, flush, args.steps)
-    n_net, n_fb = sim.stress_stats()
-    sim.set_stress_mode(L.STRESS_PLAIN)
-    sur.close()
+    # timed on a fresh copy of the workload over the same substeps as the
+    # plain line (W warm-up, then K timed from the start of the run)
+    import torch
+    from mpm_cuda_b200.sim import Simulation
+    timed, _ = build_workload(args.workload, 0, 1)
+    try:
+        with Simulation(timed, device=sim.device, kernel_config=sim.kernel_config()) as s2:
+            s2.set_stress_mode(L.STRESS_SURROGATE, sur)
+            s2.step(args.warmup)
+            s2.synchronize()
+            t_ms = time_substeps(s2, torch.cuda.ExternalStream(s2.stream_ptr(), device=sim.device), flush,
+                                 args.steps)
+            n_net, n_fb = s2.stress_stats()
+    except L.MPMError as e:
+        return {"unavailable": f"the timed run with the learned stress failed: {e}"}
+    finally:
+        sur.close()
     n_part = sum(s.n_particles for s in scenes)
     ms = t_ms / args.steps
     return {"value": n_part * args.steps / (t_ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
@@ -240,7 +256,7 @@ def surrogate_leg(args, sim, scenes, stream, flush, plain_ms_per_step: float):
             "network_share_timed": n_net / max(1, n_net + n_fb), "train_loss": loss,
             "harvest_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 3),
             "how": "BF16 MLP 10-64-64-9 (SiLU) trained on the GPU from F harvested at substeps "
-                   f"{SURROGATE_HARVEST[0]}+{SURROGATE_HARVEST[1]}k (k=1..{SURROGATE_HARVEST[2]}) of a plain run; "
+                   f"{hv[0]}+{hv[1]}k (k=1..{hv[2]}) of a plain run; "
                    "error = aggregate relative Kirchhoff stress error vs the SVD path on a later held-out "
                    "snapshot; timed like the plain line (same K, W, L2 flush)"}
 
@@ -312,35 +328,43 @@ def run_ours(args, rank, world, local_rank, dist):
                 "substep_frac": round(sub_bytes / (t_max_s / args.steps) / 1e9 / peak, 4)}
 
     # end to end through the public API: every substep's positions reach host
-    # memory inside the timed region.  Pipelined: substep k+1 is enqueued
-    # before the host waits for substep k's copy (mpm_get_positions_async), so
-    # the copy overlaps the next substep; the host then reads step k's result.
-    e2e_steps = min(args.steps, 200)
+    # memory inside the timed region.  Pipelined: two substeps are in flight
+    # (mpm_get_positions_async), so each copy overlaps the following substeps;
+    # the host reads every substep's result.  Run on a fresh copy of the
+    # workload (W warm-up substeps, then K timed from the start of the run,
+    # like the device line), so the length of the earlier runs does not matter.
+    e2e_steps = args.steps
     d = scenes[0].dim
-    host = [torch.empty((n_part, d), dtype=torch.float32, pin_memory=True).numpy() for _ in range(2)]
+    host = [torch.empty((n_part, d), dtype=torch.float32, pin_memory=True).numpy() for _ in range(3)]
+    e2e_scenes, _ = build_workload(args.workload, rank, world)
+    s3 = Simulation(e2e_scenes, device=local_rank, p2g_mode=mode, kernel_config=kcfg)
+    s3.step(args.warmup)
+    s3.synchronize()
     if dist is not None:
         dist.barrier()
     t0 = time.perf_counter()
-    prev, checksum = None, 0.0
+    tickets, checksum = [], 0.0
     for k in range(e2e_steps):
-        sim.step_async(1)
-        ticket = sim.positions_async(host[k % 2], scene=-1)
-        if prev is not None:
-            sim.wait_positions(prev)
-            checksum += float(host[(k - 1) % 2][-1, 0])
-        prev = ticket
-    sim.wait_positions(prev)
-    checksum += float(host[(e2e_steps - 1) % 2][-1, 0])
-    sim.synchronize()
+        s3.step_async(1)
+        tickets.append(s3.positions_async(host[k % 3], scene=-1))
+        if k >= 2:  # two substeps in flight: the host reads substep k - 2
+            s3.wait_positions(tickets[k - 2])
+            checksum += float(host[(k - 2) % 3][-1, 0])
+    for k in range(max(0, e2e_steps - 2), e2e_steps):
+        s3.wait_positions(tickets[k])
+        checksum += float(host[k % 3][-1, 0])
+    s3.synchronize()
     e2e_t = reduce_max(dist, time.perf_counter() - t0, device=f"cuda:{local_rank}")
+    s3.close()
     sur = None
     if world == 1 and not args.no_surrogate:
         sur = surrogate_leg(args, sim, scenes, stream, flush, t_max_s * 1e3 / args.steps)
     e2e = {"value": total_particles * e2e_steps / e2e_t, "unit": UNIT,
            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(n_part * d * 4),
            "how": "every substep: mpm_step_async(h, 1), mpm_get_positions_async of all positions into "
-                  "page-locked host memory, then mpm_wait_positions for the previous substep's copy and a host "
-                  "read of it; wall clock (the reference's loop copies positions to the host every substep); "
+                  "page-locked host memory, then mpm_wait_positions for the copy of two substeps earlier and a "
+                  "host read of it (two substeps in flight); K substeps after W warm-up on a fresh copy of the "
+                  "workload; wall clock (the reference's loop copies positions to the host every substep); "
                   "state stays resident in HBM between substeps as in the reference"}
     sim.close()
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
