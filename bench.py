@@ -275,8 +275,8 @@ def run_ours(args, rank, world, local_rank, dist):
     mode = {"binned": L.P2G_ATOMIC, "direct": L.P2G_DIRECT}[args.mode]
     sim = Simulation(scenes, device=local_rank, p2g_mode=mode, kernel_config=args.kernel_config)
     kcfg = sim.kernel_config()
-    chunk, min_ctas = C.c_int(), C.c_int()
-    L.load().mpm_kernel_config_info(kcfg, C.byref(chunk), C.byref(min_ctas))
+    chunk, min_ctas, rounds = C.c_int(), C.c_int(), C.c_int()
+    L.load().mpm_kernel_config_info(kcfg, C.byref(chunk), C.byref(min_ctas), C.byref(rounds))
     stream = torch.cuda.ExternalStream(sim.stream_ptr(), device=local_rank)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
 
@@ -374,6 +374,7 @@ def run_ours(args, rank, world, local_rank, dist):
                        "active_nodes": active_nodes, "stress": "plain (SVD)", "path": args.mode,
                        "tile_fallbacks": fallbacks, "rebins": rebins,
                        "kernel_config": {"index": kcfg, "chunk": chunk.value, "min_ctas_per_sm": min_ctas.value,
+                                         "particles_per_thread": rounds.value,
                                          "chosen_by": "autotuner" if args.kernel_config < 0 else "flag"},
                        "l2": "flushed between substeps (256 MB write, outside the timed events)",
                        "parallelism": f"replicas x{world}" if args.workload != "c4" else f"scenes split over {world}"},

@@ -291,11 +291,13 @@ int mpm_profile_stages(mpm_handle *h, int n_substeps, float *out_ms, int n_out,
 int mpm_count_active_nodes(mpm_handle *h, int scene, int64_t *n);
 
 /* Launch configurations of the fused substep kernel (the autotuner's search
- * space): configuration i runs chunks of *chunk particles with *chunk threads
- * per CTA and at least *min_ctas CTAs per SM.  No reference counterpart: the
- * reference launches fixed 128-thread blocks (MPMCUDA.cu:813-815). */
+ * space): configuration i runs *chunk threads per CTA, at least *min_ctas CTAs
+ * per SM, and chunks of *chunk x *rounds particles (each thread processes
+ * *rounds particles of a chunk in turn).  Any output pointer may be NULL.  No
+ * reference counterpart: the reference launches fixed 128-thread blocks
+ * (MPMCUDA.cu:813-815). */
 int mpm_num_kernel_configs(void);
-int mpm_kernel_config_info(int config, int *chunk, int *min_ctas);
+int mpm_kernel_config_info(int config, int *chunk, int *min_ctas, int *rounds);
 int mpm_get_kernel_config(mpm_handle *h, int *config);
 int mpm_set_kernel_config(mpm_handle *h, int config);
 

@@ -96,7 +96,7 @@ EXPORTS = {
     "mpm_count_active_nodes": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]),
     "mpm_get_bin_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "mpm_num_kernel_configs": (C.c_int, []),
-    "mpm_kernel_config_info": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "mpm_kernel_config_info": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "mpm_get_kernel_config": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "mpm_set_kernel_config": (C.c_int, [C.c_void_p, C.c_int]),
     "mpm_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]),

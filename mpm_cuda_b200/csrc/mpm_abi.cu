@@ -198,11 +198,12 @@ int mpm_get_bin_stats(mpm_handle* h, int64_t* fallbacks, int64_t* rebins) {
 
 int mpm_num_kernel_configs(void) { return mpm::kNumFusedCfgs; }
 
-int mpm_kernel_config_info(int config, int* chunk, int* min_ctas) {
+int mpm_kernel_config_info(int config, int* chunk, int* min_ctas, int* rounds) {
     if (config < 0 || config >= mpm::kNumFusedCfgs)
         return fail(nullptr, MPM_ERR_INVALID, "mpm_kernel_config_info: config %d out of range", config);
     if (chunk) *chunk = mpm::kFusedCfgs[config].chunk;
     if (min_ctas) *min_ctas = mpm::kFusedCfgs[config].min_ctas;
+    if (rounds) *rounds = mpm::kFusedCfgs[config].rounds;
     return MPM_OK;
 }
 

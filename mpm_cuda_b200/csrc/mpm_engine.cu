@@ -357,7 +357,9 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     if ((rc = alloc((void**)&counters, CNT_N * sizeof(int), "counters")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&speed_max, scenes_h.size() * sizeof(unsigned), "speed maxima")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&scene_time, scenes_h.size() * sizeof(double), "scene times")) != MPM_OK) return rc;
-    list_cap = cap / kFusedCfgs[kNumFusedCfgs - 1].chunk + std::min<long long>(cap, total_blocks) + 1;
+    // per material: at most n / (particles per chunk) full chunks plus one
+    // partial chunk per non-empty block
+    list_cap = cap / kMinChunkParticles + std::min<long long>(cap, total_blocks) + 1;
     if ((rc = alloc((void**)&chunks, kMats * list_cap * sizeof(Chunk), "chunks")) != MPM_OK) return rc;
     det_key_bits = 1;
     while (det_key_bits < 64 && (1LL << det_key_bits) <= total_blocks * 64) ++det_key_bits;
@@ -419,6 +421,8 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     grid_dirty = true;
     return MPM_OK;
 }
+
+int Engine::chunk_particles() const { return kFusedCfgs[cfg].chunk * kFusedCfgs[cfg].rounds; }
 
 void Engine::set_config(int ci) {
     cfg = ci;
@@ -695,12 +699,12 @@ void Engine::enqueue_rebin(int from) {
     }
     if (dim == 3)
         k_make_chunks<3><<<grid_blocks(n_segs, 256), 256, 0, stream>>>(seg_count, seg_start, n_segs, chunks, list_cap,
-                                                                       counters + CNT_CHUNKS, kFusedCfgs[cfg].chunk,
-                                                                       scenes_d, (int)scenes_h.size());
+                                                                       counters + CNT_CHUNKS, chunk_particles(),
+                                                                       scenes_d, (int)scenes_h.size(), err_d);
     else
         k_make_chunks<2><<<grid_blocks(n_segs, 256), 256, 0, stream>>>(seg_count, seg_start, n_segs, chunks, list_cap,
-                                                                       counters + CNT_CHUNKS, kFusedCfgs[cfg].chunk,
-                                                                       scenes_d, (int)scenes_h.size());
+                                                                       counters + CNT_CHUNKS, chunk_particles(),
+                                                                       scenes_d, (int)scenes_h.size(), err_d);
     note_launch("k_make_chunks");
     if (n_particles > 0) {
         k_bin_reset<<<nb, 256, 0, stream>>>(keys[0], n_particles, mat_slots, cell_count, seg_count);
@@ -729,6 +733,7 @@ FusedArgs Engine::fused_args(int mat, bool bump) {
     A.err_word = err_d;
     A.fallback = (unsigned*)(counters + CNT_FALLBACK);
     A.speed_max = opt.adaptive_dt ? speed_max : nullptr;
+    A.rounds = kFusedCfgs[cfg].rounds;
     A.scene = scenes_h[0];
     return A;
 }

@@ -86,6 +86,8 @@ struct Engine {
     long long next_ticket = 0;
     int fused_ctas[3] = {0, 0, 0};  // persistent CTAs per material kernel
     int cfg = 1;                     // index into kFusedCfgs
+    // particles per chunk of the current configuration (CTA size x rounds)
+    int chunk_particles() const;
     bool fixed_scene = false;        // one scene, fixed dt: fused kernels take it as a parameter
     // learned stress (MPM_STRESS_SURROGATE): the network, the version of its
     // weights the graphs were captured with, per-material persistent CTAs and

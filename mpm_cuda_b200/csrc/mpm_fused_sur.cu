@@ -12,8 +12,8 @@ static constexpr auto sur_kernel() {
 }
 
 SurFn sur_fn(int ci) {
-    static_assert(kNumFusedCfgs == 8, "update the dispatch table");
-    switch (ci) {
+    static_assert(kNumFusedKernels == 8, "update the dispatch table");
+    switch (kFusedCfgs[ci].kernel) {
         case 0: return sur_kernel<0>();
         case 1: return sur_kernel<1>();
         case 2: return sur_kernel<2>();

@@ -1,6 +1,7 @@
 // Table of the fused substep kernel's instantiations for one scene source
 // (FIXED: the scene from the kernel parameters, else from the device table),
-// indexed by dimension, material and launch configuration.  Each source's
+// indexed by dimension, material and launch configuration (configurations
+// that differ only in rounds share an instantiation).  Each source's
 // table is instantiated in its own translation unit so they compile in
 // parallel.
 #pragma once
@@ -16,8 +17,8 @@ static constexpr auto fused_kernel() {
 
 template <int D, int MAT, bool FIXED>
 static FusedFn fused_for(int ci) {
-    static_assert(kNumFusedCfgs == 8, "update the dispatch table");
-    switch (ci) {
+    static_assert(kNumFusedKernels == 8, "update the dispatch table");
+    switch (kFusedCfgs[ci].kernel) {
         case 0: return fused_kernel<D, MAT, 0, FIXED>();
         case 1: return fused_kernel<D, MAT, 1, FIXED>();
         case 2: return fused_kernel<D, MAT, 2, FIXED>();

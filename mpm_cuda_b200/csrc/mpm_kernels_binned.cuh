@@ -165,7 +165,8 @@ __global__ void __launch_bounds__(256) k_make_chunks(const int* __restrict__ seg
                                                      const int* __restrict__ seg_start, long long n_segs,
                                                      Chunk* __restrict__ chunks, long long list_cap,
                                                      int* __restrict__ n_chunks, int chunk,
-                                                     const SceneParams* __restrict__ scenes, int n_scenes) {
+                                                     const SceneParams* __restrict__ scenes, int n_scenes,
+                                                     unsigned* __restrict__ err) {
     const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_segs) return;
     const int c = seg_count[s];
@@ -173,6 +174,10 @@ __global__ void __launch_bounds__(256) k_make_chunks(const int* __restrict__ seg
     const int mat = (int)(s & 3);
     const int nch = (c + chunk - 1) / chunk;
     const int at = atomicAdd(&n_chunks[mat], nch);
+    if (at + nch > list_cap) {  // cannot happen with the list sized for the smallest chunk
+        atomicOr(err, ERR_BINNING);
+        return;
+    }
     Chunk ch;
     ch.block = (int)(s >> 2);
     ch.mat = mat;
@@ -329,6 +334,7 @@ struct FusedArgs {
     unsigned* err_word;
     unsigned* fallback;  // count of particles that used global memory
     unsigned* speed_max; // adaptive dt: per scene max of |v| + wave (float bits); null when off
+    int rounds;          // particles per thread and chunk (a chunk holds CTA size x rounds)
     // the one scene of a single-scene run with a fixed dt, read by the kernels
     // built with FIXED = true from their parameters (constant bank operands,
     // no loads) instead of from `scenes`
@@ -611,36 +617,40 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
     chunk_loop<D, CHUNK, FIXED>(A, tv, touched, s_cn,
                                 [&](const Chunk& ch, const SceneParams& sc, const int* o, const float4* w, unsigned* tb) {
         unsigned speed_bits = 0u;
-        if ((int)threadIdx.x < ch.count) {
-            const long long i = (long long)ch.start + threadIdx.x;
-            float* S = pb.s;
-            const long long cap = pb.cap;
-            unsigned err = 0;
-            float x[D];
+#pragma unroll 1
+        for (int r = 0; r < A.rounds; ++r) {
+            const int li = (int)threadIdx.x + r * CHUNK;  // this round's particle of the chunk
+            if (li < ch.count) {
+                const long long i = (long long)ch.start + li;
+                float* S = pb.s;
+                const long long cap = pb.cap;
+                unsigned err = 0;
+                float x[D];
 #pragma unroll
-            for (int a = 0; a < D; ++a) x[a] = S[(P::X + a) * cap + i];
-            Stencil<D> st;
-            if (make_stencil<D>(x, sc, st, err)) {
-                G2PAcc<D> acc;
-                g2p_window<D>(st, o, w, sc, A, acc);
-                // loaded after the gather, its register peak
-                const GroupParams g = A.groups[pb.grp[i]];
-                float F[D * D], Cn[D * D], v[D], aux;
-                ElasticSVD<D> esvd;  // snow: the plasticity step's decomposition, reused by the stress
-                err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux,
-                                                MAT == SNOW ? &esvd : nullptr);
-                if (A.speed_max) speed_bits = __float_as_uint(signal_speed<D, MAT>(v, g, aux));
+                for (int a = 0; a < D; ++a) x[a] = S[(P::X + a) * cap + i];
+                Stencil<D> st;
+                if (make_stencil<D>(x, sc, st, err)) {
+                    G2PAcc<D> acc;
+                    g2p_window<D>(st, o, w, sc, A, acc);
+                    // loaded after the gather, its register peak
+                    const GroupParams g = A.groups[pb.grp[i]];
+                    float F[D * D], Cn[D * D], v[D], aux;
+                    ElasticSVD<D> esvd;  // snow: the plasticity step's decomposition, reused by the stress
+                    err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux,
+                                                    MAT == SNOW ? &esvd : nullptr);
+                    if (A.speed_max) speed_bits = max(speed_bits, __float_as_uint(signal_speed<D, MAT>(v, g, aux)));
 
-                // ---- stress + P2G of the next substep (its dt is dt_next)
-                Stencil<D> sn;
-                if (make_stencil<D>(x, sc, sn, err)) {
-                    P2GSource<D> src;
-                    if (MAT == SNOW) snow_stress_source<D>(v, Cn, esvd, aux, g, sc.dt_next, src);
-                    else particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc.dt_next, src);
-                    scatter_global<D>(sn, src, sc, o, A, tb);
+                    // ---- stress + P2G of the next substep (its dt is dt_next)
+                    Stencil<D> sn;
+                    if (make_stencil<D>(x, sc, sn, err)) {
+                        P2GSource<D> src;
+                        if (MAT == SNOW) snow_stress_source<D>(v, Cn, esvd, aux, g, sc.dt_next, src);
+                        else particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc.dt_next, src);
+                        scatter_global<D>(sn, src, sc, o, A, tb);
+                    }
                 }
+                if (err) atomicOr(A.err_word, err);
             }
-            if (err) atomicOr(A.err_word, err);
         }
         if (A.speed_max) speed_warp_reduce(speed_bits, &s_speed);
     }, [&](int si) { speed.fold(si, &s_speed, A.speed_max); });

@@ -57,79 +57,85 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
     SpeedFlush speed;
     chunk_loop<D, CHUNK>(A, tv, touched, s_cn,
                          [&](const Chunk& ch, const SceneParams& sc, const int* o, const float4* w, unsigned* tb) {
-        const long long i = (long long)ch.start + threadIdx.x;
-        float* S = pb.s;
-        const long long cap = pb.cap;
-        unsigned err = 0;
-        bool next = false;      // the particle scatters into the next substep
-        bool eligible = false;  // its group takes the network's stress
-        int gi = 0;             // its group (re-read after the network: fewer live registers)
         unsigned speed_bits = 0u;
-        float* row = sxy + threadIdx.x * XS;
-        if ((int)threadIdx.x < ch.count) {
-            gi = pb.grp[i];
-            float x[D];
+        // every thread runs every round (the network step is warp-synchronous)
+#pragma unroll 1
+        for (int r = 0; r < A.rounds; ++r) {
+            const int li = (int)threadIdx.x + r * CHUNK;  // this round's particle of the chunk
+            const long long i = (long long)ch.start + li;
+            float* S = pb.s;
+            const long long cap = pb.cap;
+            unsigned err = 0;
+            bool next = false;      // the particle scatters into the next substep
+            bool eligible = false;  // its group takes the network's stress
+            int gi = 0;             // its group (re-read after the network: fewer live registers)
+            float* row = sxy + threadIdx.x * XS;
+            if (li < ch.count) {
+                gi = pb.grp[i];
+                float x[D];
 #pragma unroll
-            for (int a = 0; a < D; ++a) x[a] = S[(P::X + a) * cap + i];
-            Stencil<D> st;
-            if (make_stencil<D>(x, sc, st, err)) {
-                G2PAcc<D> acc;
-                g2p_window<D>(st, o, w, sc, A, acc);
+                for (int a = 0; a < D; ++a) x[a] = S[(P::X + a) * cap + i];
+                Stencil<D> st;
+                if (make_stencil<D>(x, sc, st, err)) {
+                    G2PAcc<D> acc;
+                    g2p_window<D>(st, o, w, sc, A, acc);
+                    const GroupParams g = A.groups[gi];
+                    float F[D * D], Cn[D * D], v[D], aux;
+                    err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux);
+                    if (A.speed_max) speed_bits = max(speed_bits, __float_as_uint(signal_speed<D, MAT>(v, g, aux)));
+                    Stencil<D> sn;
+                    next = make_stencil<D>(x, sc, sn, err);
+                    eligible = next && g.surrogate != 0;
+                    if (eligible) mlp::features(F, det<3>(F), SA.meta, row);
+                }
+            }
+            if (!eligible) {
+#pragma unroll
+                for (int k = 0; k < mlp::IN_PAD; ++k) row[k] = 0.f;
+            }
+            __syncwarp();
+            // ---- network: 32 rows per warp, two 16-row tiles, in place
+            if (__any_sync(0xffffffffu, eligible)) {
+                mlp::forward_tile<XS>(W, sxy + w0 * XS, sxy + w0 * XS, lane);
+                mlp::forward_tile<XS>(W, sxy + (w0 + 16) * XS, sxy + (w0 + 16) * XS, lane);
+            }
+            __syncwarp();
+            if (next) {
+                // the state stored above, read back through L2
+                float x[D], v[D], Cn[D * D], F[D * D], aux = 1.f;
+#pragma unroll
+                for (int a = 0; a < D; ++a) {
+                    x[a] = __ldcg(S + (P::X + a) * cap + i);
+                    v[a] = __ldcg(S + (P::V + a) * cap + i);
+                }
+#pragma unroll
+                for (int k = 0; k < D * D; ++k) {
+                    Cn[k] = __ldcg(S + (P::C + k) * cap + i);
+                    F[k] = __ldcg(S + (P::F + k) * cap + i);
+                }
                 const GroupParams g = A.groups[gi];
-                float F[D * D], Cn[D * D], v[D], aux;
-                err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux);
-                if (A.speed_max) speed_bits = __float_as_uint(signal_speed<D, MAT>(v, g, aux));
                 Stencil<D> sn;
-                next = make_stencil<D>(x, sc, sn, err);
-                eligible = next && g.surrogate != 0;
-                if (eligible) mlp::features(F, det<3>(F), SA.meta, row);
+                make_stencil<D>(x, sc, sn, err);  // the stencil found above
+                float tau[D * D];
+                bool use = false;
+                if (eligible) {
+                    const float J = det<3>(F);
+                    use = mlp::in_envelope(F, J, SA.meta) &&
+                          mlp::tau_from_prediction(row, F, J, g.mu, g.lambda, SA.meta, tau);
+                }
+                P2GSource<D> src;
+                if (use) {
+                    source_from_tau<D>(v, Cn, tau, g, sc.dt_next, src);
+                    ++n_net;
+                } else {
+                    particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc.dt_next, src);
+                    ++n_svd;
+                }
+                scatter_global<D>(sn, src, sc, o, A, tb);
             }
+            if (err) atomicOr(A.err_word, err);
+            __syncwarp();  // the rows are rewritten by the next round
         }
-        if (!eligible) {
-#pragma unroll
-            for (int k = 0; k < mlp::IN_PAD; ++k) row[k] = 0.f;
-        }
-        __syncwarp();
-        // ---- network: 32 rows per warp, two 16-row tiles, in place
-        if (__any_sync(0xffffffffu, eligible)) {
-            mlp::forward_tile<XS>(W, sxy + w0 * XS, sxy + w0 * XS, lane);
-            mlp::forward_tile<XS>(W, sxy + (w0 + 16) * XS, sxy + (w0 + 16) * XS, lane);
-        }
-        __syncwarp();
-        if (next) {
-            // the state stored above, read back through L2
-            float x[D], v[D], Cn[D * D], F[D * D], aux = 1.f;
-#pragma unroll
-            for (int a = 0; a < D; ++a) {
-                x[a] = __ldcg(S + (P::X + a) * cap + i);
-                v[a] = __ldcg(S + (P::V + a) * cap + i);
-            }
-#pragma unroll
-            for (int k = 0; k < D * D; ++k) {
-                Cn[k] = __ldcg(S + (P::C + k) * cap + i);
-                F[k] = __ldcg(S + (P::F + k) * cap + i);
-            }
-            const GroupParams g = A.groups[gi];
-            Stencil<D> sn;
-            make_stencil<D>(x, sc, sn, err);  // the stencil found above
-            float tau[D * D];
-            bool use = false;
-            if (eligible) {
-                const float J = det<3>(F);
-                use = mlp::in_envelope(F, J, SA.meta) &&
-                      mlp::tau_from_prediction(row, F, J, g.mu, g.lambda, SA.meta, tau);
-            }
-            P2GSource<D> src;
-            if (use) {
-                source_from_tau<D>(v, Cn, tau, g, sc.dt_next, src);
-                ++n_net;
-            } else {
-                particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc.dt_next, src);
-                ++n_svd;
-            }
-            scatter_global<D>(sn, src, sc, o, A, tb);
-        }
-        if (err) atomicOr(A.err_word, err);
         if (A.speed_max) speed_warp_reduce(speed_bits, &s_speed);
     }, [&](int si) { speed.fold(si, &s_speed, A.speed_max); });
     speed.flush(A.speed_max);

@@ -89,12 +89,14 @@ def test_kernel_config_table():
     assert n >= 2
     seen = set()
     for i in range(n):
-        ch, mb = C.c_int(), C.c_int()
-        assert lib.mpm_kernel_config_info(i, C.byref(ch), C.byref(mb)) == L.OK
+        ch, mb, rd = C.c_int(), C.c_int(), C.c_int()
+        assert lib.mpm_kernel_config_info(i, C.byref(ch), C.byref(mb), C.byref(rd)) == L.OK
         assert ch.value in (64, 128, 256) and ch.value * mb.value <= 2048
-        seen.add((i, ch.value, mb.value))
-    assert len(seen) == n
-    assert lib.mpm_kernel_config_info(n, None, None) == L.ERR_INVALID
+        assert rd.value in (1, 2, 4)
+        seen.add((ch.value, mb.value, rd.value))
+    assert len(seen) == n  # no duplicate configuration
+    assert any(r == 2 for _, _, r in seen)
+    assert lib.mpm_kernel_config_info(n, None, None, None) == L.ERR_INVALID
 
 
 def test_null_handle_calls_fail_cleanly():

@@ -93,6 +93,28 @@ def test_twenty_substeps_track_oracle(gpu, name, mode):
     compare(got, orc.state(), tol)
 
 
+@pytest.mark.parametrize("name", ["jello", "snow", "water"])
+def test_every_kernel_config_tracks_oracle(gpu, name):
+    """Every launch configuration of the fused kernel, including those whose
+    threads take two particles of a chunk in turn, gives the oracle's state."""
+    import ctypes as C
+    lib = L.load()
+    sc = blob_scene(3, name, seed=24, ppc=4)  # ~250 particles per block: partial second rounds
+    orc = oracle_for(sc)
+    assert orc.step(6) == 0
+    ref = orc.state()
+    rounds_seen = set()
+    for k in range(lib.mpm_num_kernel_configs()):
+        rd = C.c_int()
+        assert lib.mpm_kernel_config_info(k, None, None, C.byref(rd)) == L.OK
+        rounds_seen.add(rd.value)
+        with Simulation([sc], kernel_config=k, rebin_interval=3) as sim:
+            sim.step(6)
+            assert sim.kernel_config() == k
+            compare(sim.get_state(0), ref, {"x": 5e-6, "v": 6e-4, "C": 6e-4, "F": 4e-5, "aux": 4e-5})
+    assert rounds_seen >= {1, 2}
+
+
 @pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
 def test_multi_scene_batch_matches_single(gpu, mode):
     scs = [blob_scene(3, "jello", seed=30), blob_scene(3, "snow", seed=31, n_grid=40, h=1.0 / 40),
