@@ -489,6 +489,10 @@ std::mutex& tune_mutex() {
 // restored afterwards, so tuning does not advance the simulation.
 int Engine::autotune(int steps, float* best_ms) {
     MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    {
+        const int rc = recover_vc();  // the backup below must hold real v and C
+        if (rc != MPM_OK) return rc;
+    }
     if (steps <= 0) steps = 8;
     const size_t state_bytes = (size_t)n_planes * cap * sizeof(float);
     float* bk_state = nullptr;
@@ -528,6 +532,7 @@ int Engine::autotune(int steps, float* best_ms) {
         if (e == cudaSuccess) e = cudaMemcpyAsync(gp[cur], bk_grp, cap * sizeof(uint16_t), cudaMemcpyDeviceToDevice, stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(ids[cur], bk_id, cap * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream);
         if (e != cudaSuccess) break;
+        vc_deferred = false;  // the restored state holds real v and C
         set_config(ci);
         if ((rc = step(2)) != MPM_OK) break;  // prologue, graph capture, warm-up
         cudaEventRecord(a, stream);
@@ -558,6 +563,7 @@ int Engine::autotune(int steps, float* best_ms) {
     cudaFree(bk_state);
     cudaFree(bk_grp);
     cudaFree(bk_id);
+    vc_deferred = false;
     opt.p2g_mode = mode0;
     current_time = t0;
     current_frame = f0;
@@ -734,6 +740,7 @@ FusedArgs Engine::fused_args(int mat, bool bump) {
     A.fallback = (unsigned*)(counters + CNT_FALLBACK);
     A.speed_max = opt.adaptive_dt ? speed_max : nullptr;
     A.rounds = kFusedCfgs[cfg].rounds;
+    A.defer_vc = defer_vc_now() ? 1 : 0;
     A.scene = scenes_h[0];
     return A;
 }
@@ -872,7 +879,37 @@ int Engine::canonical_order() {
 
 // makes grid_mom hold the P2G of the current state (binned path): sorts the
 // particles into fresh chunks and scatters them straight to global memory
+// the fused kernels defer v and C unless a learned-stress kernel runs (it
+// reads back the v and C it stores)
+bool Engine::defer_vc_now() const {
+    for (int mat = 0; mat < kMats; ++mat)
+        if (mat_present[mat] && sur_kernel(mat)) return false;
+    return true;
+}
+
+// rebuilds the deferred v and C planes (k_recover_vc) before anything reads
+// them: the state download and upload, the first P2G of a state, the other
+// P2G paths, the autotuner's backup
+int Engine::recover_vc() {
+    if (!vc_deferred) return MPM_OK;
+    if (n_particles > 0) {
+        if (dim == 3)
+            k_recover_vc<3><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(cur), n_particles, groups_d,
+                                                                               scenes_d, grid_vel);
+        else
+            k_recover_vc<2><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(cur), n_particles, groups_d,
+                                                                               scenes_d, grid_vel);
+        MPM_CUDA_TRY(cudaGetLastError(), "v/C recovery launch");
+    }
+    vc_deferred = false;
+    return MPM_OK;
+}
+
 int Engine::prologue() {
+    {
+        const int rc = recover_vc();
+        if (rc != MPM_OK) return rc;
+    }
     const size_t grid_bytes = (size_t)total_blocks * 64 * sizeof(float4);
     MPM_CUDA_TRY(cudaMemsetAsync(grid_mom, 0, grid_bytes, stream), "prologue clear");
     MPM_CUDA_TRY(cudaMemsetAsync(blk_flag, 0, total_blocks * sizeof(unsigned), stream), "prologue flags");
@@ -1030,6 +1067,7 @@ int Engine::step(int n) {
             ++steps_since_rebin;
         }
     }
+    if (n > 0) vc_deferred = fused() && defer_vc_now();
     current_frame += n;
     current_time += (double)n * (scenes_h.empty() ? 0.0 : (double)scenes_h[0].dt);
     return MPM_OK;
@@ -1143,7 +1181,9 @@ int Engine::wait_positions(long long ticket) {
 
 int Engine::get_state(int scene, float* x, float* v, float* C, float* F, float* aux) {
     MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
-    int rc = unpermute_to_alt();
+    int rc = recover_vc();
+    if (rc != MPM_OK) return rc;
+    rc = unpermute_to_alt();
     if (rc != MPM_OK) return rc;
     MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
     const long long b = scene_begin[scene], n = scene_count[scene];
@@ -1169,7 +1209,9 @@ int Engine::get_state(int scene, float* x, float* v, float* C, float* F, float* 
 
 int Engine::set_state(int scene, const float* x, const float* v, const float* C, const float* F, const float* aux) {
     MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
-    int rc = unpermute_to_alt();
+    int rc = recover_vc();  // the planes this call does not overwrite keep real v and C
+    if (rc != MPM_OK) return rc;
+    rc = unpermute_to_alt();
     if (rc != MPM_OK) return rc;
     MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
     const long long b = scene_begin[scene], n = scene_count[scene];
@@ -1265,6 +1307,11 @@ int Engine::set_p2g_mode(int mode) {
     if (sur && mode != MPM_P2G_ATOMIC) {
         last_error = "mpm_set_p2g_mode: the surrogate stress runs in MPM_P2G_ATOMIC only";
         return MPM_ERR_UNSUPPORTED;
+    }
+    MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    {
+        const int rc = recover_vc();  // the other paths read v and C
+        if (rc != MPM_OK) return rc;
     }
     MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
     opt.p2g_mode = mode;
@@ -1463,6 +1510,7 @@ int Engine::profile_stages(int n, float* out_ms, int n_out, int* n_written) {
     const int w = std::min(n_out, 3);
     for (int s = 0; s < w; ++s) out_ms[s] = acc[s] / n;
     if (n_written) *n_written = w;
+    if (n > 0) vc_deferred = fused() && defer_vc_now();
     current_frame += n;
     current_time += (double)n * (double)scenes_h[0].dt;
     return MPM_OK;

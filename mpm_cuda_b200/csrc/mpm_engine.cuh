@@ -89,6 +89,11 @@ struct Engine {
     // particles per chunk of the current configuration (CTA size x rounds)
     int chunk_particles() const;
     bool fixed_scene = false;        // one scene, fixed dt: fused kernels take it as a parameter
+    // the state's v planes hold the last G2P positions and C is stale: the
+    // fused kernels deferred them (k_recover_vc rebuilds both)
+    bool vc_deferred = false;
+    bool defer_vc_now() const;
+    int recover_vc();
     // learned stress (MPM_STRESS_SURROGATE): the network, the version of its
     // weights the graphs were captured with, per-material persistent CTAs and
     // the network / fallback counters

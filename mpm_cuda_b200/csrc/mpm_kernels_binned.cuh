@@ -335,6 +335,7 @@ struct FusedArgs {
     unsigned* fallback;  // count of particles that used global memory
     unsigned* speed_max; // adaptive dt: per scene max of |v| + wave (float bits); null when off
     int rounds;          // particles per thread and chunk (a chunk holds CTA size x rounds)
+    int defer_vc;        // store the pre-advection position in the v planes and no C (k_recover_vc)
     // the one scene of a single-scene run with a fixed dt, read by the kernels
     // built with FIXED = true from their parameters (constant bank operands,
     // no loads) instead of from `scenes`
@@ -424,12 +425,14 @@ __device__ __forceinline__ void g2p_window(const Stencil<D>& st, const int* o, c
 }
 
 // Particle update after G2P (F / Jp / J, advection, new C) and store of the
-// new state; x, v, Cn, F, aux hold it on return.
+// new state; x, v, Cn, F, aux hold it on return.  defer_vc: the v planes get
+// the pre-advection position instead of v, and C is not stored; k_recover_vc
+// rebuilds both from it and the grid velocities when they are read.
 template <int D, int MAT>
 __device__ __forceinline__ unsigned update_and_store(const G2PAcc<D>& acc, const SceneParams& sc, const GroupParams& g,
                                                      float* __restrict__ S, long long cap, long long i, float* x,
                                                      float* v, float* Cn, float* F, float& aux,
-                                                     ElasticSVD<D>* keep = nullptr) {
+                                                     ElasticSVD<D>* keep = nullptr, bool defer_vc = false) {
     using P = Planes<D>;
     aux = 1.f;
     if (MAT != JELLO) aux = S[P::AUX * cap + i];
@@ -442,8 +445,10 @@ __device__ __forceinline__ unsigned update_and_store(const G2PAcc<D>& acc, const
     }
     const unsigned err = material_update<D, MAT>(acc, sc.dt, g, F, aux, keep);
     const float c4 = 4.f * sc.inv_h;
+    float x0[D];
 #pragma unroll
     for (int a = 0; a < D; ++a) {
+        x0[a] = x[a];
         v[a] = acc.v[a];
         x[a] = fmaf(sc.dt, acc.v[a], x[a]);
 #pragma unroll
@@ -452,10 +457,12 @@ __device__ __forceinline__ unsigned update_and_store(const G2PAcc<D>& acc, const
 #pragma unroll
     for (int a = 0; a < D; ++a) {
         S[(P::X + a) * cap + i] = x[a];
-        S[(P::V + a) * cap + i] = v[a];
+        S[(P::V + a) * cap + i] = defer_vc ? x0[a] : v[a];
     }
+    if (!defer_vc) {
 #pragma unroll
-    for (int k = 0; k < D * D; ++k) S[(P::C + k) * cap + i] = Cn[k];
+        for (int k = 0; k < D * D; ++k) S[(P::C + k) * cap + i] = Cn[k];
+    }
     if (MAT != WATER) {
 #pragma unroll
         for (int k = 0; k < D * D; ++k) S[(P::F + k) * cap + i] = F[k];
@@ -637,7 +644,7 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
                     float F[D * D], Cn[D * D], v[D], aux;
                     ElasticSVD<D> esvd;  // snow: the plasticity step's decomposition, reused by the stress
                     err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux,
-                                                    MAT == SNOW ? &esvd : nullptr);
+                                                    MAT == SNOW ? &esvd : nullptr, A.defer_vc != 0);
                     if (A.speed_max) speed_bits = max(speed_bits, __float_as_uint(signal_speed<D, MAT>(v, g, aux)));
 
                     // ---- stress + P2G of the next substep (its dt is dt_next)
@@ -655,6 +662,40 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
         if (A.speed_max) speed_warp_reduce(speed_bits, &s_speed);
     }, [&](int si) { speed.fold(si, &s_speed, A.speed_max); });
     speed.flush(A.speed_max);
+}
+
+// v and C of the last substep for particles whose fused pass deferred them:
+// the v planes hold the position the pass's G2P used, and grid_vel still holds
+// the velocities it gathered (the next grid update has not run), so the same
+// gather gives the same v and C = 4/h B.  A particle whose stencil left the
+// grid (the pass reported it) keeps its planes.
+template <int D>
+__global__ void __launch_bounds__(256) k_recover_vc(ParticleBuf pb, long long n, const GroupParams* __restrict__ groups,
+                                                    const SceneParams* __restrict__ scenes,
+                                                    const float4* __restrict__ grid_vel) {
+    using P = Planes<D>;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float* S = pb.s;
+    const long long cap = pb.cap;
+    const SceneParams& sc = scenes[groups[pb.grp[i]].scene];
+    float x0[D];
+#pragma unroll
+    for (int a = 0; a < D; ++a) x0[a] = S[(P::V + a) * cap + i];
+    Stencil<D> st;
+    unsigned err = 0;
+    if (!make_stencil<D>(x0, sc, st, err)) return;
+    const StencilIndex<D> ix(sc, st.base);
+    const float4* g = grid_vel + sc.node_off;
+    G2PAcc<D> acc;
+    g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) { return g[ix(ox, oy, D == 3 ? oz : 0)]; }, acc);
+    const float c4 = 4.f * sc.inv_h;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        S[(P::V + a) * cap + i] = acc.v[a];
+#pragma unroll
+        for (int b = 0; b < D; ++b) S[(P::C + a * D + b) * cap + i] = c4 * acc.B[a * D + b];
+    }
 }
 
 // Adaptive dt, once per substep after the fused pass (one thread per scene):
