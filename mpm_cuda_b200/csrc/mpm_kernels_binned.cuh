@@ -35,9 +35,9 @@ struct Chunk {
     int o[3];   // window origin: the home block's first node minus one per axis
 };
 
-// Tile layout.  3D: window 8^3; the velocity tile (float4) has strides
-// (1, 12, 96) so the 8 lanes of an LDS.128 phase (cells x 0..3, y 0..1) read
-// 8 distinct 16-byte bank groups.
+// Tile layout.  3D: window 8^3, stored densely (strides 1, 8, 64) with x
+// XOR-ed by 4 on odd y, so the 8 lanes of an LDS.128 phase (cells x 0..3,
+// y 0..1) read 8 distinct 16-byte bank groups.  2D: window 12^2, stride 12.
 template <int D>
 struct TileShape;
 
@@ -46,7 +46,8 @@ struct TileShape<3> {
     static constexpr int SIDE = 4;
     static constexpr int T = 8;
     static constexpr int N = 512;
-    static constexpr int VY = 12, VZ = 96, VN = 768;
+    static constexpr int VY = 8, VZ = 64, VN = 512;
+    static constexpr bool SWIZZLE = true;
 };
 
 template <>
@@ -55,6 +56,7 @@ struct TileShape<2> {
     static constexpr int T = 12;
     static constexpr int N = 144;
     static constexpr int VY = 12, VZ = 0, VN = 144;
+    static constexpr bool SWIZZLE = false;
 };
 
 // ------------------------------------------------------------- binning --
@@ -351,6 +353,7 @@ __device__ __forceinline__ const SceneParams& chunk_scene(const FusedArgs& A, in
 
 template <int D>
 __device__ __forceinline__ int tv_idx(int x, int y, int z) {
+    if constexpr (TileShape<D>::SWIZZLE) x ^= (y & 1) << 2;
     return x + TileShape<D>::VY * y + TileShape<D>::VZ * z;
 }
 
