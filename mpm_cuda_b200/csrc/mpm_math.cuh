@@ -71,8 +71,11 @@ MPM_HD void inverse(const float* A, float* Ai) {
 // reference's PolarSVD (MPMCUDA.cu:87-134).  The reference calls the McAdams
 // et al. (UW-Madison TR1690) FP32 routine; this is an independent routine:
 //   1. S = F^T F
-//   2. 4 cyclic Jacobi sweeps with exact rotation angles (Golub & Van Loan,
-//      Matrix Computations, Alg. 8.4.1-8.4.2), accumulating V
+//   2. up to 4 cyclic Jacobi sweeps with exact rotation angles (Golub & Van
+//      Loan, Matrix Computations, Alg. 8.4.1-8.4.2), accumulating V; after two,
+//      a sweep is skipped once the off-diagonal mass is below the FP32
+//      resolution of the diagonal (jacobi_converged; the method converges
+//      quadratically, so a near-rotation F is done after two)
 //   3. one Newton-Schulz polish of V:  V <- V (3 I - V^T V) / 2
 //   4. sort by eigenvalue, B = F V, Gram-Schmidt QR of B -> U, s
 
@@ -120,6 +123,14 @@ MPM_HD void jacobi_rotate(float* S, float* V) {
     }
 }
 
+// the off-diagonal mass of S is below the FP32 resolution of its diagonal:
+// a further sweep would change nothing at FP32 precision
+MPM_HD bool jacobi_converged(const float* S) {
+    const float off = S[1] * S[1] + S[2] * S[2] + S[5] * S[5];
+    const float dg = S[0] * S[0] + S[4] * S[4] + S[8] * S[8];
+    return off <= 1e-14f * dg;
+}
+
 MPM_HD void swap_cols_neg(float* V, float* lam, int a, int b) {
     // swap columns a and b and negate one so det V keeps its sign
 #pragma unroll
@@ -143,6 +154,7 @@ MPM_HD void svd3(const float* F, float* U, float* s, float* V) {
     for (int i = 0; i < 9; ++i) V[i] = (i % 4 == 0) ? 1.f : 0.f;
 #pragma unroll
     for (int sweep = 0; sweep < 4; ++sweep) {
+        if (sweep >= 2 && jacobi_converged(S)) break;
         jacobi_rotate<0, 1>(S, V);
         jacobi_rotate<0, 2>(S, V);
         jacobi_rotate<1, 2>(S, V);
@@ -261,7 +273,7 @@ MPM_HD void svd(const float* F, float* U, float* s, float* V) {
 //                                 + lambda J (J - 1) I.
 //
 // In 3D the left singular vectors and singular values come from the
-// eigendecomposition of B = F F^T = U diag(s^2) U^T (the same 4 cyclic Jacobi
+// eigendecomposition of B = F F^T = U diag(s^2) U^T (the same cyclic Jacobi
 // sweeps as svd3, accumulating U instead of V), so V, its polish and the
 // Gram-Schmidt step are not needed: s_i = sqrt(eig_i), and when det F < 0 the
 // smallest one is negated (the convention of the SVD: s0 >= s1 >= |s2|, the
@@ -278,6 +290,7 @@ MPM_HD void kirchhoff_fcr3(const float* F, float mu, float lambda, float* tau) {
     for (int i = 0; i < 9; ++i) U[i] = (i % 4 == 0) ? 1.f : 0.f;
 #pragma unroll
     for (int sweep = 0; sweep < 4; ++sweep) {
+        if (sweep >= 2 && jacobi_converged(S)) break;
         jacobi_rotate<0, 1>(S, U);
         jacobi_rotate<0, 2>(S, U);
         jacobi_rotate<1, 2>(S, U);
