@@ -1,16 +1,17 @@
-// Binned substep: particles sorted by home grid block, one fused kernel per
-// substep and material that gathers (G2P), updates the particle, evaluates
-// the stress and scatters (P2G) for the next substep through shared-memory
-// grid tiles, and a grid update that visits only the blocks P2G touched.
+// Binned substep: particles ordered by home grid block, one fused kernel per
+// substep and material that gathers (G2P) from a shared-memory window of the
+// grid velocities, updates the particle, evaluates the stress and scatters
+// (P2G) for the next substep with float4 reductions into global memory, and a
+// grid update that visits only the blocks P2G touched.
 //
 // Home block: the 4x4x4 node block (8x8 in 2D) that holds a particle's base
 // node at the last re-binning.  Inside a block the particles are ordered by
 // (material, rank inside their cell, cell): a warp's 32 consecutive particles
-// then sit in 32 different cells, so the 32 lanes of every shared-memory
-// scatter hit 32 different nodes, and the tile strides below put those nodes
-// in different banks.  A chunk is up to `chunk` particles of one block and one
-// material, contiguous in the sorted state.  The tile of a chunk is the node
-// window [S b - 1, S b + S + 3) per axis (S = block side): it holds the
+// then sit in 32 different cells, so the 32 lanes of every scatter hit 32
+// different nodes, and the window layout below puts the gather's nodes in
+// different banks.  A chunk is up to CTA size x rounds particles of one block
+// and one material, contiguous in the ordered state.  The window of a chunk is
+// the node range [S b - 1, S b + S + 3) per axis (S = block side): it holds the
 // stencil of every particle whose base node is within one node of the home
 // block.  Particles that drifted further since the last re-binning use global
 // memory directly, so results never depend on how stale the binning is.
@@ -23,7 +24,6 @@
 
 namespace mpm {
 
-constexpr int kMaxChunk = 256;  // largest chunk (particles per fused CTA)
 constexpr int kMats = 3;        // JELLO, SNOW, WATER
 
 struct Chunk {
