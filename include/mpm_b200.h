@@ -140,9 +140,10 @@ typedef struct mpm_options {
     int device;         /* CUDA device ordinal */
     int rebin_interval; /* substeps between re-binnings of the particles
                            (MPM_P2G_ATOMIC); 0 = tuned default */
-    int kernel_config;  /* fused-kernel launch configuration (chunk size and
-                           CTAs per SM, see mpm_num_kernel_configs); -1 =
-                           choose with the autotuner at creation */
+    int kernel_config;  /* fused-kernel launch configuration (threads per
+                           CTA, CTAs per SM, particles per thread; see
+                           mpm_kernel_config_info); -1 = choose with the
+                           autotuner at creation */
     int adaptive_dt;    /* MPM_P2G_ATOMIC only: each scene's dt becomes its
                            largest; every substep picks the next from the CFL
                            bound cfl * h / max(|v| + material wave speed), on
