@@ -282,6 +282,7 @@ def run_ours(args, rank, world, local_rank, dist):
 
     sim.step(args.warmup)
     sim.synchronize()
+    _, rebins_before = sim.bin_stats()
     if dist is not None:
         dist.barrier()
     with ClockSampler(local_rank) as clk:
@@ -306,7 +307,8 @@ def run_ours(args, rank, world, local_rank, dist):
         stage_names = ["rebin", "grid_update", "g2p2g"]
         alg = {"rebin": n_part * 2 * sp, "grid_update": active_nodes * 32,
                "g2p2g": n_part * 2 * sp + active_nodes * 32}
-        launches_per_step = 2  # grid update + one fused kernel per material present
+        # grid update + one fused kernel per material present
+        launches_per_step = 1 + len({g.material.type for sc in scenes for g in sc.groups})
     else:
         stage_names = ["p2g", "grid_update", "g2p"]
         alg = {"p2g": n_part * sp + active_nodes * 16, "grid_update": active_nodes * 32,
@@ -379,7 +381,8 @@ def run_ours(args, rank, world, local_rank, dist):
                        "l2": "flushed between substeps (256 MB write, outside the timed events)",
                        "parallelism": f"replicas x{world}" if args.workload != "c4" else f"scenes split over {world}"},
             "roofline": roofline, "e2e": e2e, "surrogate": sur,
-            "gpu_launches": launches_per_step * args.steps + 10 * (args.steps // 16 + 1),
+            # 7 kernels per re-binning: count, scan (2), place, chunk lists, reset, counter
+            "gpu_launches": launches_per_step * args.steps + 7 * (rebins - rebins_before),
             "clocks": clocks}
     return line, scenes
 
