@@ -318,6 +318,27 @@ def test_set_state_mid_run_binned(gpu):
     compare(got, orc.state(), {"x": 5e-6, "v": 5e-4, "C": 5e-4, "F": 3e-5, "aux": 3e-5})
 
 
+def test_deferred_v_and_c_read_back_and_kept(gpu):
+    """The fused substep writes v and C lazily: reading the state rebuilds them
+    (a second read gives the same bits), an upload of x alone keeps the last
+    substep's v and C, and the run continues as the oracle's."""
+    sc = blob_scene(3, "jello", seed=93)
+    orc = oracle_for(sc)
+    with Simulation([sc], rebin_interval=4) as sim:
+        sim.step(5)
+        a = sim.get_state(0)
+        b = sim.get_state(0)
+        for k in ("x", "v", "C", "F", "aux"):
+            assert np.array_equal(a[k], b[k]), k
+        sim.set_state(0, x=a["x"])
+        c = sim.get_state(0)
+        assert np.array_equal(c["v"], a["v"]) and np.array_equal(c["C"], a["C"])
+        sim.step(3)
+        got = sim.get_state(0)
+    assert orc.step(8) == 0
+    compare(got, orc.state(), {"x": 5e-6, "v": 6e-4, "C": 6e-4, "F": 4e-5, "aux": 4e-5})
+
+
 def _mixed_scene(seed):
     a = blob_scene(3, "jello", seed=seed)
     for name, shift in (("snow", 4), ("water", -4)):
