@@ -524,7 +524,12 @@ int Engine::autotune(int steps, float* best_ms) {
     cudaEvent_t a = nullptr, b = nullptr;
     if (e == cudaSuccess) e = cudaEventCreate(&a);
     if (e == cudaSuccess) e = cudaEventCreate(&b);
-    for (int ci = 0; ci < kNumFusedCfgs && e == cudaSuccess && rc == MPM_OK; ++ci) {
+    // two passes over the configurations, each keeping its faster time: a
+    // single short timing on a shared GPU can pick a configuration that is
+    // several per cent slower
+    std::vector<float> best_of(kNumFusedCfgs, 1e30f);
+    for (int it = 0; it < 2 * kNumFusedCfgs && e == cudaSuccess && rc == MPM_OK; ++it) {
+        const int ci = it % kNumFusedCfgs;
         e = cudaMemcpyAsync(st[cur], bk_state, state_bytes, cudaMemcpyDeviceToDevice, stream);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(scenes_d, bk_scenes.data(), bk_scenes.size() * sizeof(SceneParams),
@@ -541,11 +546,13 @@ int Engine::autotune(int steps, float* best_ms) {
         e = cudaEventSynchronize(b);
         float ms = 0.f;
         if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
-        if (e == cudaSuccess && ms < best_t) {
-            best_t = ms;
+        if (e == cudaSuccess) best_of[ci] = std::min(best_of[ci], ms);
+    }
+    for (int ci = 0; ci < kNumFusedCfgs; ++ci)
+        if (best_of[ci] < best_t) {
+            best_t = best_of[ci];
             best = ci;
         }
-    }
     if (a) cudaEventDestroy(a);
     if (b) cudaEventDestroy(b);
     // restore
