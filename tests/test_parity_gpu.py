@@ -93,13 +93,13 @@ def test_twenty_substeps_track_oracle(gpu, name, mode):
     compare(got, orc.state(), tol)
 
 
-@pytest.mark.parametrize("name", ["jello", "snow", "water"])
-def test_every_kernel_config_tracks_oracle(gpu, name):
+@pytest.mark.parametrize("d,name", [(3, "jello"), (3, "snow"), (3, "water"), (2, "jello")])
+def test_every_kernel_config_tracks_oracle(gpu, d, name):
     """Every launch configuration of the fused kernel, including those whose
     threads take two particles of a chunk in turn, gives the oracle's state."""
     import ctypes as C
     lib = L.load()
-    sc = blob_scene(3, name, seed=24, ppc=4)  # ~250 particles per block: partial second rounds
+    sc = blob_scene(d, name, seed=24, ppc=4)  # 3D: ~250 particles per block: partial second rounds
     orc = oracle_for(sc)
     assert orc.step(6) == 0
     ref = orc.state()

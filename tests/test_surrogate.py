@@ -4,6 +4,8 @@ against the SVD path, and the fused substep with the network against the
 plain substep."""
 import os
 
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -164,7 +166,8 @@ def test_trained_network_stress_error(trained, harvested):
 
 
 @pytest.mark.gpu
-def test_untrained_network_always_falls_back(surrogate_cls, gpu):
+@pytest.mark.parametrize("config", [1, 9], ids=["one-round", "two-round"])
+def test_untrained_network_always_falls_back(surrogate_cls, gpu, config):
     from mpm_cuda_b200 import _lib as L
     from mpm_cuda_b200.sim import Simulation
     from helpers import TOL_STEP, compare
@@ -178,7 +181,10 @@ def test_untrained_network_always_falls_back(surrogate_cls, gpu):
                                         center=np.full(3, 0.5))
     sc = Scene(dim=3, n=(32,) * 3, h=h, dt=1e-4, groups=[group_from_arrays(mat, h, 2, x, v, C_, F, aux)],
                bc_type=L.BC_SLIP, bc_lo=3, bc_hi=3, gravity=(0.0, -9.8, 0.0))
-    with Simulation([sc]) as plain, Simulation([sc]) as sim:
+    rounds = C.c_int()
+    assert L.load().mpm_kernel_config_info(config, None, None, C.byref(rounds)) == L.OK
+    assert rounds.value == (1 if config == 1 else 2)
+    with Simulation([sc], kernel_config=config) as plain, Simulation([sc], kernel_config=config) as sim:
         sim.set_stress_mode(L.STRESS_SURROGATE, sur)
         plain.step(3)
         sim.step(3)
