@@ -12,8 +12,8 @@
 // is U diag(f(sigma)) U^T, exact for the constructed F.  Training runs on the
 // GPU: a warp-level forward + backward pass (mma.sync BF16 tensor cores, FP32
 // accumulation), split-K weight-gradient GEMMs on the same tensor cores, and
-// Adam on FP32 master weights.  The plain path's kirchhoff_fcr judges the
-// trained network's stress error (mpm_surrogate_eval).
+// Adam on FP32 master weights.  The plain path's kirchhoff_fcr is the
+// reference for the trained network's stress error (mpm_surrogate_eval).
 #include "mpm_b200.h"
 
 #include <cuda_bf16.h>

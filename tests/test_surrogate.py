@@ -161,7 +161,7 @@ def test_trained_network_stress_error(trained, harvested):
     print(f"loss {loss:.3e} accepted {ok.mean():.4f} stress error: network {err_net:.4%} series only {err_series:.4%}")
     assert err_net <= 0.01
     assert err_net < 0.5 * err_series
-    # the SVD path judges against the FP64 oracle too
+    # the SVD path itself agrees with the FP64 oracle
     assert agg_rel(tr[ok], M.fcr_tau(held[ok], 1.0, lam_mu)) < 1e-4
 
 
