@@ -318,6 +318,26 @@ def test_set_state_mid_run_binned(gpu):
     compare(got, orc.state(), {"x": 5e-6, "v": 5e-4, "C": 5e-4, "F": 3e-5, "aux": 3e-5})
 
 
+def test_dense_scene_fills_the_chunk_lists(gpu):
+    """A small grid filled at 8 particles per cell needs the most chunks per
+    block (here ~2,200 64-particle chunks for 512 blocks); the configurations
+    with the smallest and with two-round chunks both track the oracle."""
+    h, n = 1.0 / 32, 32
+    lo, hi = [4 * h] * 3, [28 * h] * 3
+    x = S.jitter_fill(lo, hi, h, 8, S.box(lo, hi), np.random.default_rng(7))
+    g = S.make_group(S.water(), x, h, 8, (0.0, 0.0, 0.0))
+    sc = Scene(dim=3, n=(n,) * 3, h=h, dt=1e-4, groups=[g], bc_type=L.BC_SLIP, bc_lo=3, bc_hi=3,
+               gravity=(0.0, -9.8, 0.0))
+    orc = oracle_for(sc)
+    assert orc.step(2) == 0
+    ref = orc.state()
+    for k in (3, 10):  # 64 threads x 1 round, 64 threads x 2 rounds
+        with Simulation([sc], kernel_config=k) as sim:
+            sim.step(2)
+            assert sim.device_errors() == 0
+            compare(sim.get_state(0), ref, {"x": 5e-6, "v": 5e-4, "C": 5e-4, "F": 3e-5, "aux": 3e-5})
+
+
 def test_deferred_v_and_c_read_back_and_kept(gpu):
     """The fused substep writes v and C lazily: reading the state rebuilds them
     (a second read gives the same bits), an upload of x alone keeps the last
