@@ -1041,6 +1041,9 @@ int Engine::step(int n) {
             if (rc != MPM_OK) return rc;
         }
         const int run = opt.rebin_interval - 1;  // plain substeps between two re-binnings
+        // set after every launched substep, so an early return below leaves it
+        // describing the state the launched substeps produced
+        const bool defer = defer_vc_now();
         for (int i = 0; i < n; ++i) {
             const int rebin = steps_since_rebin >= opt.rebin_interval ? 1 : 0;
             if (opt.use_graph && !rebin && run > 1 && steps_since_rebin == 1 && n - i >= run) {
@@ -1050,6 +1053,7 @@ int Engine::step(int n) {
                     if (rc != MPM_OK) return rc;
                 }
                 MPM_CUDA_TRY(cudaGraphLaunch(run_graphs[cur], stream), "graph launch");
+                vc_deferred = defer;
                 steps_since_rebin += run;
                 i += run - 1;
                 continue;
@@ -1067,6 +1071,7 @@ int Engine::step(int n) {
                 if (lrc != MPM_OK) return lrc;
                 MPM_CUDA_TRY(cudaGetLastError(), "kernel launch");
             }
+            vc_deferred = defer;
             if (rebin) {
                 cur = 1 - cur;
                 steps_since_rebin = 0;
@@ -1074,7 +1079,7 @@ int Engine::step(int n) {
             ++steps_since_rebin;
         }
     }
-    if (n > 0) vc_deferred = fused() && defer_vc_now();
+    if (n > 0 && !fused()) vc_deferred = false;  // the other paths store v and C
     current_frame += n;
     current_time += (double)n * (scenes_h.empty() ? 0.0 : (double)scenes_h[0].dt);
     return MPM_OK;
