@@ -1516,13 +1516,13 @@ int Engine::profile_stages(int n, float* out_ms, int n_out, int* n_written) {
         }
     }
     for (auto& e : ev) cudaEventDestroy(e);
+    if (n > 0) vc_deferred = fused() && defer_vc_now();
     const int lrc = take_launch_error();
     if (lrc != MPM_OK) return lrc;
     MPM_CUDA_TRY(cudaGetLastError(), "profile launch");
     const int w = std::min(n_out, 3);
     for (int s = 0; s < w; ++s) out_ms[s] = acc[s] / n;
     if (n_written) *n_written = w;
-    if (n > 0) vc_deferred = fused() && defer_vc_now();
     current_frame += n;
     current_time += (double)n * (double)scenes_h[0].dt;
     return MPM_OK;
