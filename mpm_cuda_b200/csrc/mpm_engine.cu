@@ -774,11 +774,12 @@ void Engine::enqueue_grid_update() {
     // cursors, so the fused launches append the next substep's blocks from zero
     cudaLaunchAttribute attr;
     const cudaLaunchConfig_t lc = pdl_config(update_ctas, 256, 0, stream, &attr);
-    auto k = dim == 3 ? k_grid_update_active<3> : k_grid_update_active<2>;
+    auto k = dim == 3 ? (fixed_scene ? k_grid_update_active<3, true> : k_grid_update_active<3, false>)
+                      : (fixed_scene ? k_grid_update_active<2, true> : k_grid_update_active<2, false>);
     const cudaError_t e = cudaLaunchKernelEx(&lc, k, grid_mom, grid_vel, (const int*)active, counters + CNT_ACTIVE,
                                              blk_flag, blk_epoch, (const int*)(counters + CNT_EPOCH),
                                              (const SceneParams*)scenes_d, n_scenes, counters + CNT_CURSOR, (int)kMats,
-                                             (unsigned*)(counters + CNT_UPDATE_DONE));
+                                             (unsigned*)(counters + CNT_UPDATE_DONE), scenes_h[0]);
     note_launch_status("k_grid_update_active", e);
 }
 

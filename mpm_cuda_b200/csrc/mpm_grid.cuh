@@ -108,10 +108,12 @@ template <int D>
 __device__ __forceinline__ void block_node_coords(const SceneParams& sc, long long blk, int in, int& ix,
                                                   int& iy, int& iz) {
     constexpr int S = BlockShape<D>::SIDE;
-    const int bx = (int)(blk % sc.nb[0]);
-    const long long r = blk / sc.nb[0];
-    const int by = (int)(r % sc.nb[1]);
-    const int bz = (int)(r / sc.nb[1]);
+    // 32-bit division: a scene has fewer than 2^31 nodes, so fewer than 2^25 blocks
+    const int lb = (int)blk;
+    const int bx = lb % sc.nb[0];
+    const int r = lb / sc.nb[0];
+    const int by = r % sc.nb[1];
+    const int bz = r / sc.nb[1];
     ix = bx * S + (in % S);
     iy = by * S + ((in / S) % S);
     iz = (D == 3) ? bz * S + in / (S * S) : 0;

@@ -281,22 +281,23 @@ __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.lau
 // Grid update of the blocks P2G touched.  The last CTA to finish resets the
 // active-block count and the fused kernels' chunk cursors for the next pass
 // (every CTA has read the count before it counts itself done).
-template <int D>
+// FIXED: the one scene of a fixed-dt run comes from the kernel parameters
+// (fixed_scene), as in the fused kernel.
+template <int D, bool FIXED>
 __global__ void __launch_bounds__(256) k_grid_update_active(float4* __restrict__ grid_mom, float4* __restrict__ grid_vel,
                                                             const int* __restrict__ active, int* __restrict__ n_active,
                                                             unsigned* __restrict__ blk_flag, int* __restrict__ blk_epoch,
                                                             const int* __restrict__ epoch,
                                                             const SceneParams* __restrict__ scenes, int n_scenes,
                                                             int* __restrict__ cursors, int n_cursors,
-                                                            unsigned* __restrict__ done) {
+                                                            unsigned* __restrict__ done, SceneParams fixed_scene) {
     pdl_wait();
     const int na = *n_active;
     const int ep = *epoch;
     const int lane = threadIdx.x & 63;
     for (int e = blockIdx.x * 4 + (threadIdx.x >> 6); e < na; e += gridDim.x * 4) {
         const int b = active[e];
-        const int s = scene_of_block(scenes, n_scenes, b);
-        const SceneParams& sc = scenes[s];
+        const SceneParams& sc = FIXED ? fixed_scene : scenes[scene_of_block(scenes, n_scenes, b)];
         int ix, iy, iz;
         block_node_coords<D>(sc, b - sc.block_off, lane, ix, iy, iz);
         const long long gi = (long long)b * 64 + lane;
