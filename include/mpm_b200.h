@@ -313,9 +313,8 @@ int mpm_autotune(mpm_handle *h, int n_substeps, int *chosen, float *ms_per_subst
 int mpm_get_bin_stats(mpm_handle *h, int64_t *fallbacks, int64_t *rebins);
 
 /* Substeps without any device allocation, for callers that cannot allocate:
- * code running while the application captures a CUDA graph, plug-in hosts
- * with a fixed device memory budget, loops that forbid allocator calls after
- * start-up.  No counterpart in the reference (its step() uses grids that its
+ * plug-in hosts with a fixed device memory budget, loops that forbid
+ * allocator calls after start-up.  No counterpart in the reference (its step() uses grids that its
  * constructor allocated).
  * Runs n_substeps of ONE scene with exactly one particle group (material,
  * p_mass, p_vol from scene->groups[0]; its particle pointers are ignored)

@@ -1,11 +1,9 @@
 // mpm_step_noalloc: the substep for callers that must not allocate device
 // memory.
 //
-// Some callers cannot call cudaMalloc at all: code that runs while a CUDA
-// graph of the surrounding application is being captured (an allocation
-// there breaks the capture), plug-in hosts that hand out a fixed device
-// memory budget up front, and real-time loops that forbid allocator calls
-// after start-up.  For them this entry point runs whole substeps of one scene
+// Some callers cannot call cudaMalloc at all: plug-in hosts that hand out a
+// fixed device memory budget up front, and real-time loops that forbid
+// allocator calls after start-up.  For them this entry point runs whole substeps of one scene
 // whose particle state lives in device memory the caller already owns.  The
 // only other memory it touches is one fixed scratch area compiled into this
 // library: the scene's grid (momentum and velocity) and an error word.

@@ -1,9 +1,8 @@
 """mpm_step_noalloc: substeps for callers that cannot allocate device memory.
 
-Some callers of this library cannot call cudaMalloc: code that runs while the
-surrounding application captures a CUDA graph, plug-in hosts that hand out a
-fixed device memory budget, real-time loops that forbid allocator calls after
-start-up.  mpm_step_noalloc serves them: it steps a scene whose particle state
+Some callers of this library cannot call cudaMalloc: plug-in hosts that hand
+out a fixed device memory budget, real-time loops that forbid allocator calls
+after start-up.  mpm_step_noalloc serves them: it steps a scene whose particle state
 lives in device memory the caller already owns, and keeps the grid in a fixed
 scratch array compiled into the library.  These tests check it against the
 handle-based entry point (mpm_create + mpm_step) on two calls in a row, and
