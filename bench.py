@@ -1,17 +1,20 @@
 """Benchmark of the MPM substep: particle-substeps/s on one or more B200s.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c3]
                     [--impl ours|reference]
 
 A step is one explicit MPM substep (P2G with stress, grid update, G2P with
 the F update and advection) over every particle of the workload, state
-resident in HBM.  The default workload is the 3D jello scene: 128^3 grid,
-0.3 cube at 8 particles/cell (~453k particles), E = 5e4, nu = 0.3,
+resident in HBM.  The default workload is the 256^3 3D jello scene on which
+the learned-stress comparison and the comparison with the reference build are
+stated: 256^3 grid, dx = 1/256, a 0.245 cube centred at (0.5, 0.6, 0.5) at 8
+particles/cell (~1.97M particles), v = (0, -2, 0), E = 5e4, nu = 0.3,
 rho = 1000, dt = 1e-4, slip walls 3 cells wide; synthetic seeded particles
-(no dataset exists for this scene).
+(no dataset exists for this scene).  --workload c1 runs the 128^3 jello scene
+(0.3 cube, ~453k particles), c2 the 256^3 snow scene, c4 the 64 batched scenes.
 
 Multi-GPU (torchrun, one process per GPU): every rank simulates its own
-replica of the workload (c1) or its share of the 64 batched scenes (c4); the
+replica of the workload (c1, c2, c3) or its share of the 64 batched scenes (c4); the
 path has no exchange step, so there is no data-path collective ("weak"
 scaling).  Timing: CUDA events on the simulation's stream around every
 substep, L2 flushed (256 MB write) between substeps outside the events,
@@ -20,7 +23,8 @@ max over ranks.
 --impl reference runs the reference's own substep (MPMSimulator::step() of
 MPMCUDA.cu, built unmodified into oracle/_ref/libmpm_ref.so) on the same
 scene through its own code path (FP64 state, host syncs and a device-to-host
-position copy every substep).
+position copy every substep).  Its time varies between runs on a shared box,
+so it is timed three times on the same simulation and the median is reported.
 """
 from __future__ import annotations
 
@@ -48,6 +52,8 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # at the fixed dt = 1e-4, hardening makes some snow scenes break the CFL bound.
 SURROGATE_HARVEST = (1400, 200, 8, 350)
 SURROGATE_HARVEST_BY_WORKLOAD = {"c4": (100, 50, 6, 100)}
+# timings of the reference arm (median reported)
+REF_REPEATS = 3
 
 
 def hbm_peak():
@@ -409,7 +415,8 @@ def run_reference(args):
     steps = min(args.steps, 200)
     warm = min(args.warmup, 20)
     sim.step(warm)
-    ms = sim.time_steps(steps)
+    repeats = [sim.time_steps(steps) for _ in range(REF_REPEATS)]
+    ms = statistics.median(repeats)
     sim.close()
     n = sc.n_particles
     value = n * steps / (ms * 1e-3)
@@ -417,9 +424,11 @@ def run_reference(args):
             "warmup": warm, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": {"workload": desc, "particles_per_gpu": n,
+                       "repeats_ms_per_step": [round(r / steps, 4) for r in repeats],
                        "note": "reference MPMSimulator::step() (MPMCUDA.cu:793-925) built unmodified for sm_100a; "
                                "its stock path: FP64 state, 3 device syncs and a D2H position copy per substep; "
-                               "its hard-coded 10h walls and constants"},
+                               "its hard-coded 10h walls and constants; median of "
+                               f"{REF_REPEATS} timings of {steps} consecutive substeps"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                              "sample": f"{steps} substeps of {desc}; the reference implementation of this path "
                                        "is CUDA, so it runs on the B200 driven by one host thread"},
@@ -431,7 +440,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--workload", default="c1", choices=["c0", "c1", "c2", "c3", "c3big", "c4"])
+    ap.add_argument("--workload", default="c3", choices=["c0", "c1", "c2", "c3", "c3big", "c4"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="binned", choices=["binned", "direct"])
     ap.add_argument("--kernel-config", type=int, default=-1, help="fused-kernel configuration; -1 = autotune")

@@ -50,10 +50,11 @@ enum mpm_boundary_type {
 /* P2G reduction modes */
 enum mpm_p2g_mode {
     MPM_P2G_ATOMIC = 0,        /* particles binned by grid block; one fused
-                                  G2P + stress + P2G kernel per substep with
-                                  shared-memory grid tiles flushed by FP32
-                                  vector atomics (fast; summation order varies
-                                  run to run) */
+                                  G2P + stress + P2G kernel per substep that
+                                  gathers from a shared-memory window of the
+                                  grid velocities and scatters with FP32
+                                  vector reductions to global memory (fast;
+                                  summation order varies run to run) */
     MPM_P2G_DETERMINISTIC = 1, /* cell-sorted gather reduction: bitwise
                                   identical results across runs */
     MPM_P2G_DIRECT = 2         /* unbinned: one thread per particle, stencil
@@ -327,8 +328,12 @@ int mpm_get_bin_stats(mpm_handle *h, int64_t *fallbacks, int64_t *rebins);
  * rejected with MPM_ERR_INVALID.  Every call shares that scratch, so calls
  * whose work overlaps on the GPU race.  The first call on a device looks up the
  * scratch address with that device current; make it before any stream
- * capture begins.  Waits for the stream and returns MPM_ERR_SIM if the device
- * error word is set.  Calls no cudaMalloc, cudaFree or allocating routine. */
+ * capture begins.  The address is kept per device ordinal for the life of the
+ * process: it belongs to the context current at that first call (the device's
+ * primary context for runtime-API callers), so later calls must run in that
+ * context, and it is not looked up again after a cudaDeviceReset.  Waits for
+ * the stream and returns MPM_ERR_SIM if the device error word is set.  Calls
+ * no cudaMalloc, cudaFree or allocating routine. */
 int mpm_step_noalloc(const mpm_scene_desc *scene, float *state, int64_t plane_stride,
                      int64_t n_particles, int n_substeps, void *stream);
 

@@ -1068,6 +1068,9 @@ int Engine::step(int n) {
             } else {
                 if (rebin) enqueue_rebin(cur);
                 enqueue_fused_substep(rebin ? 1 - cur : cur);
+                // kernels of this substep may be queued even if a launch
+                // below reports an error
+                vc_deferred = defer;
                 const int lrc = take_launch_error();
                 if (lrc != MPM_OK) return lrc;
                 MPM_CUDA_TRY(cudaGetLastError(), "kernel launch");

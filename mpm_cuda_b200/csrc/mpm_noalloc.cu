@@ -18,7 +18,10 @@
 //     streams, two host threads) race on the grid and give wrong results;
 //   * the first call on a device looks up the array's device address with that
 //     device current (cudaGetSymbolAddress); make that first call before any
-//     stream capture begins;
+//     stream capture begins.  The address is kept per device ordinal for the
+//     life of the process and belongs to the context current at that first call
+//     (the device's primary context for runtime-API callers): later calls must
+//     run in that context, and a cudaDeviceReset does not refresh it;
 //   * each call clears the grid and the error word it uses, so nothing carries
 //     over from the previous call except what the caller's state holds.
 #include "mpm_b200.h"
