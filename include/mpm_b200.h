@@ -38,8 +38,9 @@ enum mpm_material_type { MPM_JELLO = 0, MPM_SNOW = 1, MPM_WATER = 2, MPM_SAND = 
 
 /* Wall treatment of the grid update (VelUpdate, MPMCUDA.cu:459-469).
  * A node with index i along an axis is a lower-wall node if i < bc_lo and an
- * upper-wall node if i >= n - bc_hi.  The reference 3D build corresponds to
- * MPM_BC_SLIP with bc_lo = 11, bc_hi = 10 (its 10h band, MPMCUDA.cu:845-850). */
+ * upper-wall node if i >= n - bc_hi.  The reference 3D build's walls are a
+ * position test instead (MPMCUDA.cu:462-469, band 10 h, :845-850): set
+ * mpm_scene_desc.ref_band = 10 with MPM_BC_SLIP to reproduce it exactly. */
 enum mpm_boundary_type {
     MPM_BC_STICKY = 0,   /* zero all velocity components of a wall node */
     MPM_BC_SLIP = 1,     /* zero the wall-normal component */
@@ -131,6 +132,15 @@ typedef struct mpm_scene_desc {
                           reference DBL_EPSILON (MPMCUDA.cu:444) */
     int n_groups;
     const mpm_group_desc *groups;
+    double ref_band;   /* > 0: the walls are the reference's position test with
+                          a band of ref_band cells (MPMCUDA.cu:462-469 with
+                          lower = origin + band h, upper = origin + n h - band h,
+                          :845-850): node i of an axis is a wall node when
+                          origin + i h <= lower or >= upper, evaluated in FP64
+                          with the reference's own operations, so a node the
+                          reference's rounding puts outside the band (e.g.
+                          n - 10 for n = 48, h = 1/48) is outside here too;
+                          bc_lo / bc_hi are then ignored.  0: bc_lo / bc_hi. */
 } mpm_scene_desc;
 
 typedef struct mpm_options {
@@ -300,6 +310,13 @@ int mpm_count_active_nodes(mpm_handle *h, int scene, int64_t *n);
  * (MPMCUDA.cu:813-815). */
 int mpm_num_kernel_configs(void);
 int mpm_kernel_config_info(int config, int *chunk, int *min_ctas, int *rounds);
+/* How a configuration orders and scatters the particles: *cell_major = 1 when
+ * the re-binning puts a cell's particles together (else rank-major: a warp's
+ * lanes in distinct cells); *segmented = 1 when the lanes of a warp that share
+ * a stencil base are summed in shared memory before one reduction per node
+ * (else every particle reduces its own 3^D node values).  The reference
+ * scatters every particle's values with FP64 atomics (MPMCUDA.cu:388-421). */
+int mpm_kernel_config_scatter(int config, int *cell_major, int *segmented);
 int mpm_get_kernel_config(mpm_handle *h, int *config);
 int mpm_set_kernel_config(mpm_handle *h, int config);
 

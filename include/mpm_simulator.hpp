@@ -161,9 +161,11 @@ struct ObjInitInfo {
 class MPMSimulator {
    public:
     struct Options {
-        // wall band of the reference's VelUpdate: components zeroed at nodes with
-        // index <= 10 or >= n - 10 (MPMCUDA.cu:845-850, 467-469)
+        // wall band of the reference's VelUpdate: the normal component zeroed at
+        // nodes within 10 h of a wall by its FP64 position test (MPMCUDA.cu:845-850,
+        // 462-469); ref_band = 0 uses the node-count thresholds bc_lo / bc_hi
         int bc_type = MPM_BC_SLIP;
+        double ref_band = 10.0;
         int bc_lo = 11, bc_hi = 10;
         double gravity_y = -9.8;           // MPMSimulator.cpp:186
         double mass_eps = 2.220446049250313e-16;  // MPMCUDA.cu:444
@@ -234,6 +236,7 @@ class MPMSimulator {
         sc.bc_type = opt.bc_type;
         sc.bc_lo = opt.bc_lo;
         sc.bc_hi = opt.bc_hi;
+        sc.ref_band = opt.ref_band;
         sc.mass_eps = opt.mass_eps;
         sc.n_groups = (int)groups.size();
         sc.groups = groups.data();

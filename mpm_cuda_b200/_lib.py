@@ -42,7 +42,7 @@ class SceneDesc(C.Structure):
     _fields_ = [("dim", C.c_int), ("n", C.c_int * 3), ("h", C.c_double), ("origin", C.c_double * 3),
                 ("dt", C.c_double), ("gravity", C.c_double * 3), ("bc_type", C.c_int),
                 ("bc_lo", C.c_int), ("bc_hi", C.c_int), ("mass_eps", C.c_double),
-                ("n_groups", C.c_int), ("groups", C.POINTER(GroupDesc))]
+                ("n_groups", C.c_int), ("groups", C.POINTER(GroupDesc)), ("ref_band", C.c_double)]
 
 
 class Options(C.Structure):
@@ -97,6 +97,7 @@ EXPORTS = {
     "mpm_get_bin_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "mpm_num_kernel_configs": (C.c_int, []),
     "mpm_kernel_config_info": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "mpm_kernel_config_scatter": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "mpm_get_kernel_config": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "mpm_set_kernel_config": (C.c_int, [C.c_void_p, C.c_int]),
     "mpm_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]),

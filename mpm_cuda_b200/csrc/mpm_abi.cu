@@ -207,6 +207,14 @@ int mpm_kernel_config_info(int config, int* chunk, int* min_ctas, int* rounds) {
     return MPM_OK;
 }
 
+int mpm_kernel_config_scatter(int config, int* cell_major, int* segmented) {
+    if (config < 0 || config >= mpm::kNumFusedCfgs)
+        return fail(nullptr, MPM_ERR_INVALID, "mpm_kernel_config_scatter: config %d out of range", config);
+    if (cell_major) *cell_major = mpm::kFusedCfgs[config].order == mpm::ORDER_CELL ? 1 : 0;
+    if (segmented) *segmented = mpm::kFusedCfgs[config].scatter == mpm::SCATTER_SEGMENTED ? 1 : 0;
+    return MPM_OK;
+}
+
 int mpm_get_kernel_config(mpm_handle* h, int* config) {
     if (!h || !config) return fail(h, MPM_ERR_INVALID, "mpm_get_kernel_config: bad argument");
     *config = h->eng.cfg;

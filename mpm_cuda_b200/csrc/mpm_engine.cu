@@ -157,7 +157,8 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
             std::snprintf(buf, sizeof(buf), "mpm_create: scene %d needs h > 0 and dt > 0", s);
             return bad(MPM_ERR_INVALID, buf);
         }
-        if (d.bc_type < MPM_BC_STICKY || d.bc_type > MPM_BC_SEPARATE || d.bc_lo < 0 || d.bc_hi < 0)
+        if (d.bc_type < MPM_BC_STICKY || d.bc_type > MPM_BC_SEPARATE || d.bc_lo < 0 || d.bc_hi < 0 ||
+            !(d.ref_band >= 0.0))
             return bad(MPM_ERR_INVALID, "mpm_create: bad boundary descriptor");
         if (d.n_groups < 0 || (d.n_groups > 0 && !d.groups)) return bad(MPM_ERR_INVALID, "mpm_create: bad group list");
         for (int gi = 0; gi < d.n_groups; ++gi) {
@@ -204,8 +205,10 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
         sp.inv_h = (float)(1.0 / d.h);
         sp.dt = (float)d.dt;
         sp.bc_type = d.bc_type;
-        sp.bc_lo = d.bc_lo;
-        sp.bc_hi = d.bc_hi;
+        for (int a = 0; a < 3; ++a) {
+            sp.bc_lo[a] = sp.bc_hi[a] = 0;
+            if (a < dim) axis_walls(sp.n[a], d.h, d.origin[a], d.ref_band, d.bc_lo, d.bc_hi, sp.bc_lo[a], sp.bc_hi[a]);
+        }
         sp.mass_eps = (float)d.mass_eps;
         sp.n_blocks = (long long)sp.nb[0] * sp.nb[1] * sp.nb[2];
         sp.block_off = block_off;
@@ -426,10 +429,15 @@ int Engine::chunk_particles() const { return kFusedCfgs[cfg].chunk * kFusedCfgs[
 
 void Engine::set_config(int ci) {
     cfg = ci;
+    const int dyn = fused_dyn_smem(dim, kFusedCfgs[ci].kernel);
     for (int mat = 0; mat < kMats; ++mat) {
         int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_fn(dim, mat, ci, fixed_scene), kFusedCfgs[ci].chunk, 0) !=
-            cudaSuccess) {
+        const FusedFn fn = fused_fn(dim, mat, ci, fixed_scene);
+        // the segmented scatter's staging buffer can exceed the 48 KB a kernel
+        // gets without opting in; a failure here shows in the occupancy query
+        if (dyn > 0 && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) != cudaSuccess)
+            cudaGetLastError();
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kFusedCfgs[ci].chunk, dyn) != cudaSuccess) {
             cudaGetLastError();  // the query failed: fall back to one CTA per SM
             per_sm = 1;
         }
@@ -682,8 +690,8 @@ void Engine::enqueue_direct_substep() {
 }
 
 // bins the particles of buffer `from` by (home block, material) into the
-// other buffer, rank-major within each segment (counting placement, no sort),
-// and builds the chunk lists of the result
+// other buffer, in the configuration's order within each segment (counting
+// placement, no sort), and builds the chunk lists of the result
 void Engine::enqueue_rebin(int from) {
     const int to = 1 - from;
     const long long n_segs = total_blocks * 4;
@@ -704,10 +712,10 @@ void Engine::enqueue_rebin(int from) {
     if (n_particles > 0) {
         if (dim == 3)
             k_bin_place<3><<<nb, 256, 0, stream>>>(buf(from), buf(to), n_particles, keys[0], rank, cell_count,
-                                                   seg_count, seg_start, mat_slots, err_d);
+                                                   seg_count, seg_start, mat_slots, kFusedCfgs[cfg].order, err_d);
         else
             k_bin_place<2><<<nb, 256, 0, stream>>>(buf(from), buf(to), n_particles, keys[0], rank, cell_count,
-                                                   seg_count, seg_start, mat_slots, err_d);
+                                                   seg_count, seg_start, mat_slots, kFusedCfgs[cfg].order, err_d);
         note_launch("k_bin_place");
     }
     if (dim == 3)
@@ -796,7 +804,8 @@ void Engine::enqueue_g2p2g(int parity) {
             note_launch("k_g2p2g_sur");
         } else {
             cudaLaunchAttribute attr;
-            const cudaLaunchConfig_t lc = pdl_config(fused_ctas[mat], kFusedCfgs[cfg].chunk, 0, stream, &attr);
+            const cudaLaunchConfig_t lc = pdl_config(fused_ctas[mat], kFusedCfgs[cfg].chunk,
+                                                     fused_dyn_smem(dim, kFusedCfgs[cfg].kernel), stream, &attr);
             const cudaError_t e = cudaLaunchKernelEx(&lc, fused_fn(dim, mat, cfg, fixed_scene), buf(parity), A);
             note_launch_status("k_g2p2g", e);
             note_launch("fused_fn");

@@ -1,7 +1,7 @@
 // Table of the fused substep kernel's instantiations for one scene source
 // (FIXED: the scene from the kernel parameters, else from the device table),
 // indexed by dimension, material and launch configuration (configurations
-// that differ only in rounds share an instantiation).  Each source's
+// that differ only in rounds or particle order share an instantiation).  Each source's
 // table is instantiated in its own translation unit so they compile in
 // parallel.
 #pragma once
@@ -10,14 +10,14 @@
 
 namespace mpm {
 
-template <int D, int MAT, int CI, bool FIXED>
+template <int D, int MAT, int K, bool FIXED>
 static constexpr auto fused_kernel() {
-    return &k_g2p2g<D, MAT, kFusedCfgs[CI].chunk, kFusedCfgs[CI].min_ctas, FIXED>;
+    return &k_g2p2g<D, MAT, kFusedKernels[K].chunk, kFusedKernels[K].min_ctas, FIXED, kFusedKernels[K].scatter>;
 }
 
 template <int D, int MAT, bool FIXED>
 static FusedFn fused_for(int ci) {
-    static_assert(kNumFusedKernels == 8, "update the dispatch table");
+    static_assert(kNumFusedKernels == 12, "update the dispatch table");
     switch (kFusedCfgs[ci].kernel) {
         case 0: return fused_kernel<D, MAT, 0, FIXED>();
         case 1: return fused_kernel<D, MAT, 1, FIXED>();
@@ -26,7 +26,11 @@ static FusedFn fused_for(int ci) {
         case 4: return fused_kernel<D, MAT, 4, FIXED>();
         case 5: return fused_kernel<D, MAT, 5, FIXED>();
         case 6: return fused_kernel<D, MAT, 6, FIXED>();
-        default: return fused_kernel<D, MAT, 7, FIXED>();
+        case 7: return fused_kernel<D, MAT, 7, FIXED>();
+        case 8: return fused_kernel<D, MAT, 8, FIXED>();
+        case 9: return fused_kernel<D, MAT, 9, FIXED>();
+        case 10: return fused_kernel<D, MAT, 10, FIXED>();
+        default: return fused_kernel<D, MAT, 11, FIXED>();
     }
 }
 

@@ -7,6 +7,8 @@
 // on a few contiguous 1 KB runs.
 #pragma once
 
+#include <cmath>
+
 #include "mpm_types.cuh"
 
 namespace mpm {
@@ -82,8 +84,8 @@ __device__ __forceinline__ float4 grid_node_update(float4 g, const SceneParams& 
     bool lo[3], hi[3], any = false;
 #pragma unroll
     for (int a = 0; a < D; ++a) {
-        lo[a] = id[a] < sc.bc_lo;
-        hi[a] = id[a] >= sc.n[a] - sc.bc_hi;
+        lo[a] = id[a] < sc.bc_lo[a];
+        hi[a] = id[a] >= sc.n[a] - sc.bc_hi[a];
         any |= lo[a] | hi[a];
     }
     if (sc.bc_type == BC_STICKY) {
@@ -101,6 +103,30 @@ __device__ __forceinline__ float4 grid_node_update(float4 g, const SceneParams& 
     }
     if (D == 2) v[2] = 0.f;
     return make_float4(v[0], v[1], v[2], m);
+}
+
+// Wall thresholds of one axis (host): bc_lo / bc_hi as given, or, with
+// ref_band > 0, the nodes the reference's FP64 position test marks
+// (MPMCUDA.cu:462-469): node i sits at fma(i, h, origin) (the kernel's
+// origin + i * h, contracted), the bounds are origin + band * h and
+// (origin + h * n) - band * h, each operation rounded once as in the
+// reference's host code (MPMCUDA.cu:845-850).  The marked nodes are a prefix
+// and a suffix of the axis (positions increase with i).
+inline void axis_walls(int n, double h, double origin, double ref_band, int bc_lo, int bc_hi, int& lo, int& hi) {
+    if (!(ref_band > 0.0)) {
+        lo = bc_lo;
+        hi = bc_hi;
+        return;
+    }
+    const volatile double bh = ref_band * h;  // volatile: no contraction into an FMA
+    const volatile double nh = h * (double)n;
+    const volatile double top = origin + nh;
+    const double lower = origin + bh;
+    const double upper = top - bh;
+    lo = 0;
+    while (lo < n && std::fma((double)lo, h, origin) <= lower) ++lo;
+    hi = 0;
+    while (hi < n && std::fma((double)(n - 1 - hi), h, origin) >= upper) ++hi;
 }
 
 // coordinates of node `in` (0..63) of block `blk` of scene `sc`

@@ -79,9 +79,10 @@ __device__ __forceinline__ void home_of(const SceneParams& sc, const float* x, l
 }
 
 // Binning by counting, without a sort.  The particles of each (home block,
-// material) segment are ordered rank-major: first every cell's rank-0
-// particle (cells ascending), then every rank-1 particle, and so on, so the
-// lanes of a warp sit in distinct cells.
+// material) segment are ordered rank-major (first every cell's rank-0
+// particle, cells ascending, then every rank-1 particle, and so on, so the
+// lanes of a warp sit in distinct cells) or cell-major (cells ascending, a
+// cell's particles together).
 
 // Pass 1: home block b, cell c and material m of every particle, its rank
 // among the particles of (b, m, c) and the size of segment (b, m).
@@ -105,19 +106,19 @@ __global__ void __launch_bounds__(256) k_bin_count(ParticleBuf pb, long long n, 
     key[i] = ((unsigned long long)b << 8) | ((unsigned long long)g.type << 6) | (unsigned long long)c;
 }
 
-// Pass 2 (after the scan of the segment sizes): the slot of particle (r, c)
-// in its segment is
+// Pass 2 (after the scan of the segment sizes): with n_c' the segment's cell
+// counts, the slot of particle (r, c) in its segment is, rank-major,
 //   sum over cells c' of min(n_c', r)   (particles of lower rank)
 // + #{c' < c : n_c' > r}                (rank r in lower cells),
-// n_c' the segment's cell counts; the particle's state moves there.  Ranks
-// are exact, so the slots are a permutation of the segment; a slot outside
-// it (inconsistent counts) is reported, not written.
+// and, cell-major, sum over c' < c of n_c' + r; the particle's state moves
+// there.  Ranks are exact, so the slots are a permutation of the segment; a
+// slot outside it (inconsistent counts) is reported, not written.
 template <int D>
 __global__ void __launch_bounds__(256) k_bin_place(ParticleBuf src, ParticleBuf dst, long long n,
                                                    const unsigned long long* __restrict__ key,
                                                    const int* __restrict__ rank, const int* __restrict__ cell_count,
                                                    const int* __restrict__ seg_count,
-                                                   const int* __restrict__ seg_start, MatSlots ms,
+                                                   const int* __restrict__ seg_start, MatSlots ms, int cell_major,
                                                    unsigned* __restrict__ err) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -126,7 +127,7 @@ __global__ void __launch_bounds__(256) k_bin_place(ParticleBuf src, ParticleBuf 
     const int m = (int)((k >> 6) & 3), c = (int)(k & 63);
     const int r = rank[i];
     const int4* cnt = reinterpret_cast<const int4*>(cell_count + (b * ms.n + ms.s[m]) * 64);
-    int lower = 0, before = 0;
+    int lower = 0, before = 0, cells_below = 0;
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
         const int4 v = cnt[q];
@@ -135,9 +136,10 @@ __global__ void __launch_bounds__(256) k_bin_place(ParticleBuf src, ParticleBuf 
         for (int t = 0; t < 4; ++t) {
             lower += min(nc[t], r);
             before += (4 * q + t < c && nc[t] > r) ? 1 : 0;
+            cells_below += (4 * q + t < c) ? nc[t] : 0;
         }
     }
-    const int off = lower + before;
+    const int off = cell_major ? cells_below + r : lower + before;
     const int seg = (int)(b * 4 + m);
     if (off < 0 || off >= seg_count[seg]) {
         atomicOr(err, ERR_BINNING);
@@ -528,6 +530,95 @@ __device__ __forceinline__ void mark_touched(unsigned touched, const SceneParams
     }
 }
 
+// ---- segmented scatter (SCATTER_SEGMENTED)
+//
+// P2G of a warp's particles with one reduction per (run of lanes sharing a
+// stencil base, node) instead of one per (lane, node).  In cell-major order
+// the particles of a cell are consecutive, so the lanes of a warp form a few
+// runs (about 4 at 8 particles per cell) whose members scatter into the same
+// 3^D nodes.  Each lane writes its 3^D node values to its column of the
+// warp's staging buffer V[row = node][column = lane]; then lane `row` walks
+// the columns in order, summing the values of row `row` over each run, and at
+// a run's last column reduces the sum into that run's node `row` of the grid
+// (red.global.add.v4.f32).  The walk is the same for every lane (run limits
+// are warp-uniform bit masks), so it has no divergence.  Lanes whose stencil
+// left the chunk's window scatter directly to global memory and do not take
+// part; a lane whose base differs from its neighbour's starts a new run, so
+// results do not depend on the order.  Every lane of the warp must call this.
+
+// staging-buffer slot of (row, column): the column XOR-ed with the row's low
+// three bits, so a column write (fixed row, 32 lanes) and a row read (fixed
+// column, one row per lane) both touch distinct 16-byte bank groups
+__device__ __forceinline__ int seg_slot(int row, int col) { return row * 32 + (col ^ (row & 7)); }
+
+template <int D>
+__device__ __forceinline__ void scatter_segmented(bool valid, const Stencil<D>& sn, const P2GSource<D>& src,
+                                                  const SceneParams& sc, const int* o, const FusedArgs& A,
+                                                  unsigned* touched, float4* __restrict__ V) {
+    constexpr int R = seg_rows(D);
+    constexpr int S = BlockShape<D>::SHIFT;
+    constexpr int M = BlockShape<D>::SIDE - 1;
+    constexpr int SIDE = BlockShape<D>::SIDE;
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const bool inw = valid && in_window<D>(sn.base, o);
+    if (valid && !inw) {
+        atomicAdd(A.fallback, 1u);
+        p2g_global<D>(sn, src, sc, A.grid_mom, A.blk_flag, A.active, A.n_active);
+    }
+    const unsigned part = __ballot_sync(FULL, inw);
+    if (part == 0u) return;
+    // stencil base in window coordinates (0 .. T - 3 per axis, 4 bits each)
+    const int l0 = sn.base[0] - o[0], l1 = sn.base[1] - o[1], l2 = D == 3 ? sn.base[2] - o[2] : 0;
+    const int key = inw ? l0 + 16 * (l1 + 16 * l2) : -1;
+    if (inw) {
+        p2g_scatter<D>(sn, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 c) {
+            V[seg_slot(D == 3 ? (ox * 3 + oy) * 3 + oz : ox * 3 + oy, lane)] = c;
+        });
+    }
+    const int kprev = __shfl_up_sync(FULL, key, 1);
+    const bool head = inw && (lane == 0 || kprev != key);
+    const unsigned heads = __ballot_sync(FULL, head);
+    if (head) atomicOr(touched, touched_bits<D>(l0, l1, l2));
+    const unsigned ends = part & ~((part & ~heads) >> 1);  // the next lane does not continue the run
+    __syncwarp();
+    // this lane's row: stencil node (rx, ry, rz)
+    const int row = lane;
+    const bool has_row = row < R;
+    const int rx = D == 3 ? row / 9 : row / 3, ry = D == 3 ? (row / 3) % 3 : row % 3, rz = D == 3 ? row % 3 : 0;
+    const int px = o[0] + rx, py = o[1] + ry, pz = o[2] + rz;
+    const int sy = sc.nb[0] * 64, sz = sc.nb[0] * sc.nb[1] * 64;
+    float4* g = A.grid_mom + sc.node_off;
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int m = 0; m < 32; ++m) {
+        if (!((part >> m) & 1u)) continue;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (has_row) v = V[seg_slot(row, m)];
+        if ((heads >> m) & 1u) {
+            acc = v;
+        } else {
+            acc.x += v.x;
+            acc.y += v.y;
+            acc.z += v.z;
+            acc.w += v.w;
+        }
+        if ((ends >> m) & 1u) {
+            const int km = __shfl_sync(FULL, key, m);
+            if (has_row) {
+                const int gx = px + (km & 15), gy = py + ((km >> 4) & 15);
+                int idx = (gx >> S) * 64 + (gx & M) + (gy >> S) * sy + (gy & M) * SIDE;
+                if (D == 3) {
+                    const int gz = pz + (km >> 8);
+                    idx += (gz >> S) * sz + (gz & M) * SIDE * SIDE;
+                }
+                atomicAdd(&g[idx], acc);
+            }
+        }
+    }
+    __syncwarp();  // the buffer is rewritten by the next call
+}
+
 // Per-CTA maximum of the particles' signal speed |v| + wave for adaptive dt:
 // warps reduce into a shared word during a chunk, thread 0 folds it into a
 // running maximum of the current scene after the chunk and sends one global
@@ -608,10 +699,12 @@ __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][T
 // velocity tile, F / Jp / J update, advection, stress, and P2G of the next
 // substep (MPMCUDA.cu:310-741 in one pass: the reference runs P2G, VelUpdate
 // and InterpolateAndMove as three kernels with full-grid sweeps and host
-// syncs between them).  The P2G scatter reduces straight to global memory
-// with float4 vector reductions (red.global.add.v4.f32).  FIXED: the scene
-// comes from A.scene (one scene, dt fixed for the run).
-template <int D, int MAT, int CHUNK, int MINB, bool FIXED>
+// syncs between them).  The P2G scatter reduces into global memory with
+// float4 vector reductions (red.global.add.v4.f32), per particle
+// (SCATTER_DIRECT) or per run of a warp's lanes sharing a stencil base
+// (SCATTER_SEGMENTED, staging buffer in dynamic shared memory).  FIXED: the
+// scene comes from A.scene (one scene, dt fixed for the run).
+template <int D, int MAT, int CHUNK, int MINB, bool FIXED, int SCATTER>
 __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs A) {
     using P = Planes<D>;
     using TS = TileShape<D>;
@@ -619,6 +712,8 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
     __shared__ unsigned touched[2];                 // 3^D neighbour-block bits
     __shared__ int s_cn[2];
     __shared__ unsigned s_speed;                    // adaptive dt: this chunk's max signal speed
+    extern __shared__ __align__(16) float4 seg_stage[];  // SCATTER_SEGMENTED: per-warp staging buffers
+    float4* V = seg_stage + (threadIdx.x >> 5) * (seg_rows(D) * 32);
 
     pdl_wait();     // the grid update ahead of this launch has finished
     pdl_trigger();  // the next pass may launch; it waits for this one to end
@@ -631,6 +726,13 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
 #pragma unroll 1
         for (int r = 0; r < A.rounds; ++r) {
             const int li = (int)threadIdx.x + r * CHUNK;  // this round's particle of the chunk
+            // SCATTER_SEGMENTED: sn and src are scattered after the particle's
+            // branch, by every lane of the warp together; SCATTER_DIRECT
+            // scatters inside it (fewer live registers across the branch)
+            bool scatter = false;
+            Stencil<D> sn;
+            P2GSource<D> src;
+            if constexpr (SCATTER == SCATTER_SEGMENTED) sn.base[0] = sn.base[1] = sn.base[2] = 0;
             if (li < ch.count) {
                 const long long i = (long long)ch.start + li;
                 float* S = pb.s;
@@ -652,16 +754,16 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
                     if (A.speed_max) speed_bits = max(speed_bits, __float_as_uint(signal_speed<D, MAT>(v, g, aux)));
 
                     // ---- stress + P2G of the next substep (its dt is dt_next)
-                    Stencil<D> sn;
                     if (make_stencil<D>(x, sc, sn, err)) {
-                        P2GSource<D> src;
                         if (MAT == SNOW) snow_stress_source<D>(v, Cn, esvd, aux, g, sc.dt_next, src);
                         else particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc.dt_next, src);
-                        scatter_global<D>(sn, src, sc, o, A, tb);
+                        if constexpr (SCATTER == SCATTER_SEGMENTED) scatter = true;
+                        else scatter_global<D>(sn, src, sc, o, A, tb);
                     }
                 }
                 if (err) atomicOr(A.err_word, err);
             }
+            if constexpr (SCATTER == SCATTER_SEGMENTED) scatter_segmented<D>(scatter, sn, src, sc, o, A, tb, V);
         }
         if (A.speed_max) speed_warp_reduce(speed_bits, &s_speed);
     }, [&](int si) { speed.fold(si, &s_speed, A.speed_max); });

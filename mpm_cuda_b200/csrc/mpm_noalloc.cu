@@ -217,7 +217,8 @@ extern "C" int mpm_step_noalloc(const mpm_scene_desc* scene, float* state, int64
     if (n_particles < 0 || n_substeps < 0 || (n_particles > 0 && !state) || plane_stride < n_particles)
         return fail(MPM_ERR_INVALID, "mpm_step_noalloc: bad state pointer, particle count or plane stride");
     if (!(d.h > 0.0) || !(d.dt > 0.0)) return fail(MPM_ERR_INVALID, "mpm_step_noalloc: needs h > 0 and dt > 0");
-    if (d.bc_type < MPM_BC_STICKY || d.bc_type > MPM_BC_SEPARATE || d.bc_lo < 0 || d.bc_hi < 0)
+    if (d.bc_type < MPM_BC_STICKY || d.bc_type > MPM_BC_SEPARATE || d.bc_lo < 0 || d.bc_hi < 0 ||
+        !(d.ref_band >= 0.0))
         return fail(MPM_ERR_INVALID, "mpm_step_noalloc: bad boundary descriptor");
     const mpm_group_desc& gd = d.groups[0];
     const mpm_material_desc& m = gd.material;
@@ -250,8 +251,10 @@ extern "C" int mpm_step_noalloc(const mpm_scene_desc* scene, float* state, int64
     sc.inv_h = (float)(1.0 / d.h);
     sc.dt = (float)d.dt;
     sc.bc_type = d.bc_type;
-    sc.bc_lo = d.bc_lo;
-    sc.bc_hi = d.bc_hi;
+    for (int a = 0; a < 3; ++a) {
+        sc.bc_lo[a] = sc.bc_hi[a] = 0;
+        if (a < dim) axis_walls(sc.n[a], d.h, d.origin[a], d.ref_band, d.bc_lo, d.bc_hi, sc.bc_lo[a], sc.bc_hi[a]);
+    }
     sc.mass_eps = (float)d.mass_eps;
     sc.node_off = 0;
     sc.block_off = 0;

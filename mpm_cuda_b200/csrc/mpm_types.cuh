@@ -33,7 +33,8 @@ struct SceneParams {
     float origin[3];
     float dt;  // current substep (grid update, G2P, advection)
     float gravity[3];
-    int bc_type, bc_lo, bc_hi;
+    int bc_type;
+    int bc_lo[3], bc_hi[3];  // per axis: node i is a wall node if i < bc_lo or i >= n - bc_hi
     float mass_eps;
     long long node_off;  // first node of the scene in the global grid arrays
     long long n_nodes;

@@ -70,6 +70,9 @@ class Scene:
     bc_hi: int = 3
     mass_eps: float = 2.220446049250313e-16
     name: str = ""
+    # > 0: walls from the reference's FP64 position test with this band in
+    # cells (bc_lo / bc_hi ignored); see mpm_scene_desc.ref_band
+    ref_band: float = 0.0
 
     @property
     def n_particles(self) -> int:
@@ -123,6 +126,7 @@ def scene_descs(scenes: Sequence[Scene]):
             sd.gravity = (C.c_double * 3)(*gr[:3])
             sd.bc_type, sd.bc_lo, sd.bc_hi = s.bc_type, s.bc_lo, s.bc_hi
             sd.mass_eps = s.mass_eps
+            sd.ref_band = s.ref_band
             sd.n_groups = len(s.groups)
             sd.groups = gdescs
     return sdescs, keep

@@ -27,7 +27,7 @@ _DP = C.POINTER(C.c_double)
 class OrcGrid(C.Structure):
     _fields_ = [("dim", C.c_int), ("n", C.c_int * 3), ("h", C.c_double), ("origin", C.c_double * 3),
                 ("dt", C.c_double), ("gravity", C.c_double * 3), ("bc_type", C.c_int),
-                ("bc_lo", C.c_int), ("bc_hi", C.c_int), ("mass_eps", C.c_double)]
+                ("bc_lo", C.c_int), ("bc_hi", C.c_int), ("mass_eps", C.c_double), ("ref_band", C.c_double)]
 
 
 class OrcGroup(C.Structure):
@@ -95,7 +95,7 @@ class OracleSim:
 
     def __init__(self, dim: int, n: Sequence[int], h: float, dt: float, groups: List[OGroup],
                  x, v, C_, F, aux, group=None, origin=(0, 0, 0), gravity=(0, -9.8, 0),
-                 bc_type=BC_SLIP, bc_lo=3, bc_hi=3, mass_eps=2.220446049250313e-16):
+                 bc_type=BC_SLIP, bc_lo=3, bc_hi=3, mass_eps=2.220446049250313e-16, ref_band=0.0):
         self.lib = load()
         self.dim = dim
         N = x.shape[0]
@@ -126,7 +126,7 @@ class OracleSim:
         nn = list(n) + [1] * (3 - len(n))
         self.grid = OrcGrid(dim, (C.c_int * 3)(*nn[:3]), h, (C.c_double * 3)(*list(origin)[:3]), dt,
                             (C.c_double * 3)(*(list(gravity) + [0, 0, 0])[:3]), bc_type, bc_lo, bc_hi,
-                            mass_eps)
+                            mass_eps, ref_band)
         self.groups = (OrcGroup * len(groups))(*[
             OrcGroup(g.type, g.mu, g.lam, g.xi, g.theta_c, g.theta_s, g.bulk_k, g.gamma, g.p_mass, g.p_vol)
             for g in groups])
@@ -158,6 +158,14 @@ class OracleSim:
             elif self.groups[gi].type == WATER:
                 out[m] = self.J[m]
         return out
+
+    def grid_update(self, mass: np.ndarray, mom: np.ndarray) -> np.ndarray:
+        """The oracle's grid update (MPMCUDA.cu:435-472) on given node masses
+        and momenta of this scene's grid; returns the node velocities (G, 3)."""
+        m = np.ascontiguousarray(mass, np.float64).copy()
+        v = np.ascontiguousarray(mom, np.float64).reshape(-1).copy()
+        self.lib.orc_grid_update(C.byref(self.grid), _dp(m), _dp(v))
+        return v.reshape(-1, 3)
 
     def grid_mass(self):
         return self.mass.reshape(self.nn[::-1]) if self.dim == 3 else self.mass.reshape(self.nn[1], self.nn[0])

@@ -327,8 +327,22 @@ int orc_grid_update(const orc_grid *g, double *grid_mass, double *grid_mom) {
         long id[3] = {i % nx, (i / nx) % ny, i / (nx * ny)};
         int lo[3], hi[3], any = 0;
         for (int a = 0; a < d; ++a) {
-            lo[a] = id[a] < g->bc_lo;
-            hi[a] = id[a] >= g->n[a] - g->bc_hi;
+            if (g->ref_band > 0.0) {
+                /* MPMCUDA.cu:462-469: node position origin + idx * h (a fused
+                 * multiply-add in the reference's kernel) against the bounds
+                 * origin + band h and origin + h n - band h, which the
+                 * reference's host code computes one rounded operation at a
+                 * time (MPMCUDA.cu:845-850) */
+                volatile double bh = g->ref_band * g->h;
+                volatile double top = g->origin[a] + g->h * (double)g->n[a];
+                const double lower = g->origin[a] + bh, upper = top - bh;
+                const double pos = fma((double)id[a], g->h, g->origin[a]);
+                lo[a] = pos <= lower;
+                hi[a] = pos >= upper;
+            } else {
+                lo[a] = id[a] < g->bc_lo;
+                hi[a] = id[a] >= g->n[a] - g->bc_hi;
+            }
             any |= lo[a] | hi[a];
         }
         if (g->bc_type == ORC_BC_STICKY) {

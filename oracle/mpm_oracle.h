@@ -56,6 +56,9 @@ typedef struct {
     int bc_lo;          /* node index i is a lower-wall node if i < bc_lo */
     int bc_hi;          /* node index i is an upper-wall node if i >= n - bc_hi */
     double mass_eps;    /* nodes with mass <= mass_eps get zero velocity */
+    double ref_band;    /* > 0: walls by the reference's FP64 position test with a
+                           band of ref_band cells (MPMCUDA.cu:462-469, 845-850);
+                           bc_lo / bc_hi are then ignored */
 } orc_grid;
 
 typedef struct {

@@ -19,6 +19,27 @@ TOL_STEP = {"x": 2e-6, "v": 1e-4, "C": 1e-4, "F": 1e-5, "aux": 1e-5}
 TOL_REF = {1: {"x": 1e-6, "v": 1e-4, "C": 1e-4, "F": 1e-4, "aux": 1e-4},
            10: {"x": 5e-6, "v": 1e-3, "C": 1e-3, "F": 1e-3, "aux": 1e-3}}
 TOL_REF_MEDIAN = {1: 2e-6, 10: 2e-5}
+# Snow's F: the reference's FP32 SVD of the plasticity clamp (MPMCUDA.cu:
+# 638-660, svd3_cuda.h) returns singular vectors off by up to ~3e-4 for a few clamped
+# particles (one of 531 in the lower-wall fixture, whose singular values agree
+# to 5e-6); the maximum is bounded there and the 99th percentile tightly.
+TOL_REF_SNOW_F_MAX = {1: 5e-4, 10: 1e-3}
+TOL_REF_SNOW_F_P99 = {1: 1e-5, 10: 2e-4}
+
+
+def golden_tolerance(material_type: int, k: int) -> dict:
+    """Per-field maximum tolerances against a reference-build fixture after
+    k substeps for a group of the given material."""
+    tol = dict(TOL_REF[k])
+    if material_type == L.SNOW:
+        tol["F"] = TOL_REF_SNOW_F_MAX[k]
+    return tol
+
+
+def check_snow_f_percentile(got_F, ref_F, k: int):
+    d = np.abs(np.asarray(got_F, np.float64) - ref_F).reshape(len(ref_F), -1).max(axis=1)
+    p99 = float(np.percentile(d, 99) / max(np.abs(ref_F).max(), 1e-30))
+    assert p99 < TOL_REF_SNOW_F_P99[k], f"snow F 99th percentile error {p99:.3e} after {k} substeps"
 
 
 def group_from_arrays(mat: MaterialParams, h: float, ppc: int, x, v, C, F, aux) -> Group:
@@ -48,7 +69,7 @@ def oracle_for(scene: Scene) -> ocpu.OracleSim:
     return ocpu.OracleSim(d, scene.n, scene.h, scene.dt, [oracle_group(g) for g in scene.groups], cat(xs),
                           cat(vs), cat(Cs), cat(Fs), cat(auxs), group=cat(grp), origin=scene.origin,
                           gravity=scene.gravity, bc_type=scene.bc_type, bc_lo=scene.bc_lo, bc_hi=scene.bc_hi,
-                          mass_eps=scene.mass_eps)
+                          mass_eps=scene.mass_eps, ref_band=scene.ref_band)
 
 
 def rel_err(a, b):
@@ -71,3 +92,78 @@ def compare(gpu_state: dict, ref_state: dict, tol: dict, fields=("x", "v", "C", 
     bad = {k: e for k, e in errs.items() if e > tol[k]}
     assert not bad, f"errors above tolerance: {bad} (all: {errs})"
     return errs
+
+
+def reference_compat(scene: Scene) -> Scene:
+    """The scene with the reference build's hard-coded constants where they
+    differ from the scene's: its walls (the 10h slip band, MPMCUDA.cu:845-850,
+    462-469), gravity -9.8 on y (MPMSimulator.cpp:186), the snow clamp
+    [1 - 8e-2, 1 + 2e-2] and hardening 10 (MPMCUDA.cu:344, 658-660), water
+    p = 2.51 (J^-7 - 1) (MPMCUDA.cu:353)."""
+    import copy
+    s = copy.deepcopy(scene)
+    s.bc_type, s.ref_band = L.BC_SLIP, 10.0
+    s.gravity = (0.0, -9.8, 0.0)
+    s.mass_eps = 2.220446049250313e-16
+    s.origin = (0.0, 0.0, 0.0)
+    for g in s.groups:
+        m = g.material
+        if m.type == L.SNOW:
+            m.theta_c, m.theta_s, m.xi = 8e-2, 2e-2, 10.0
+        elif m.type == L.WATER:
+            m.bulk_k, m.gamma = 2.51, 7.0
+    return s
+
+
+def _field_errors(got: np.ndarray, ref: np.ndarray, absolute: bool):
+    diff = np.abs(np.asarray(got, np.float64) - np.asarray(ref, np.float64)).reshape(len(ref), -1).max(axis=1)
+    scale = 1.0 if absolute else max(float(np.abs(ref).max()), 1e-30)
+    return float(diff.max() / scale), float(np.median(diff) / scale)
+
+
+def reference_build_errors(scene: Scene, steps: int, kernel_config: int = -1, device: int = 0) -> dict:
+    """Runs the scene (a single 3D scene, reference constants applied with
+    reference_compat) for `steps` substeps through the CUDA path and through
+    the reference's own step() (oracle/_ref, FP64 state), from the same
+    float32 initial state, and returns the per-field divergence: positions
+    as max / median absolute error in cells, v and F as max / median of each
+    particle's largest component error relative to the field's largest
+    magnitude.  Needs a GPU."""
+    from oracle import ref as R
+    sc = reference_compat(scene)
+    assert sc.dim == 3
+    rs = R.RefSim(sc.h, sc.dt, sc.n)
+    for g in sc.groups:
+        m, n = g.material, g.n
+        x = np.float64(np.float32(g.x))
+        v = np.float64(np.float32(g.v)) if g.v is not None else np.tile(np.float64(np.float32(g.init_v[:3])), (n, 1))
+        F = np.float64(np.float32(g.F)) if g.F is not None else np.tile(np.eye(3), (n, 1, 1))
+        Cm = np.float64(np.float32(g.C)) if g.C is not None else np.zeros((n, 3, 3))
+        aux = np.float64(np.float32(g.aux)) if g.aux is not None else np.ones(n)
+        Fp = J = None
+        if m.type == L.SNOW:
+            Fp = np.zeros((n, 3, 3))
+            for a in range(3):
+                Fp[:, a, a] = aux ** (1.0 / 3.0)
+        if m.type == L.WATER:
+            J = aux
+        E = m.E if m.type != L.WATER else 1e4
+        nu = m.nu if m.type != L.WATER else 0.2
+        rs.add_group(m.type, E, nu, m.rho, g.p_mass, g.p_vol, x, v, F, Fp=Fp, J=J, C_=Cm)
+    rs.step(steps)
+    ref = [rs.get_group(gi) for gi in range(len(sc.groups))]
+    rs.close()
+    with Simulation([sc], device=device, kernel_config=kernel_config) as sim:
+        sim.step(steps)
+        got = sim.get_state(0)
+    cat = lambda k: np.concatenate([r[k] for r in ref])
+    out = {"substeps": steps, "particles": int(sum(g.n for g in sc.groups))}
+    ex = _field_errors(got["x"], cat("x"), absolute=True)
+    out["x_max_cells"], out["x_median_cells"] = ex[0] / sc.h, ex[1] / sc.h
+    for k in ("v", "F"):
+        e = _field_errors(got[k], cat(k), absolute=False)
+        out[f"{k}_max_rel"], out[f"{k}_median_rel"] = e
+    # the walls: the comparison holds the reference's band on both sides
+    lo, hi = np.float64(got["x"]).min(axis=0) / sc.h, np.float64(got["x"]).max(axis=0) / sc.h
+    out["min_node_distance_to_wall_band"] = float(min((lo - 11).min(), (np.asarray(sc.n) - 10 - hi).min()))
+    return out

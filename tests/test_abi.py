@@ -90,13 +90,19 @@ def test_kernel_config_table():
     seen = set()
     for i in range(n):
         ch, mb, rd = C.c_int(), C.c_int(), C.c_int()
+        cm, sg = C.c_int(), C.c_int()
         assert lib.mpm_kernel_config_info(i, C.byref(ch), C.byref(mb), C.byref(rd)) == L.OK
+        assert lib.mpm_kernel_config_scatter(i, C.byref(cm), C.byref(sg)) == L.OK
         assert ch.value in (64, 128, 256) and ch.value * mb.value <= 2048
         assert rd.value in (1, 2, 4)
-        seen.add((ch.value, mb.value, rd.value))
+        assert cm.value in (0, 1) and sg.value in (0, 1)
+        assert not (sg.value and not cm.value)  # the segmented scatter runs on cell-major chunks
+        seen.add((ch.value, mb.value, rd.value, cm.value, sg.value))
     assert len(seen) == n  # no duplicate configuration
-    assert any(r == 2 for _, _, r in seen)
+    assert any(c[2] == 2 for c in seen)
+    assert {(c[3], c[4]) for c in seen} == {(0, 0), (1, 0), (1, 1)}
     assert lib.mpm_kernel_config_info(n, None, None, None) == L.ERR_INVALID
+    assert lib.mpm_kernel_config_scatter(n, None, None) == L.ERR_INVALID
 
 
 def test_null_handle_calls_fail_cleanly():

@@ -10,7 +10,8 @@ from mpm_cuda_b200 import _lib as L
 from mpm_cuda_b200 import scenes as S
 from mpm_cuda_b200.sim import Scene, Simulation
 
-from helpers import TOL_REF, TOL_STEP, compare, group_from_arrays, oracle_for, rel_err
+from helpers import (TOL_REF, TOL_STEP, check_snow_f_percentile, compare, golden_tolerance, group_from_arrays,
+                     oracle_for, rel_err)
 
 pytestmark = pytest.mark.gpu
 
@@ -243,8 +244,9 @@ def golden_scene(z):
         groups.append(Group(material=mat, p_mass=float(z[p + "p_mass"]), p_vol=float(z[p + "p_vol"]),
                             x=z[p + "in_x"], v=z[p + "in_v"], C=z[p + "in_C"], F=z[p + "in_F"],
                             aux=z[p + "in_aux"]))
-    # the reference build's constants: 10h slip band, gravity -9.8 on y
-    return Scene(dim=3, n=(n, n, n), h=h, dt=dt, groups=groups, bc_type=L.BC_SLIP, bc_lo=11, bc_hi=10,
+    # the reference build's constants: its 10h slip band (FP64 position test),
+    # gravity -9.8 on y
+    return Scene(dim=3, n=(n, n, n), h=h, dt=dt, groups=groups, bc_type=L.BC_SLIP, ref_band=10.0,
                  gravity=(0.0, -9.8, 0.0), mass_eps=2.220446049250313e-16)
 
 
@@ -264,7 +266,10 @@ def test_matches_reference_build_golden(gpu, path, mode):
                 n = z[f"g{gi}_in_x"].shape[0]
                 ref = {f: z[f"g{gi}_s{k}_{f}"] for f in ("x", "v", "C", "F", "aux")}
                 got = {f: st[f][off:off + n] for f in st}
-                compare(got, ref, TOL_REF[k])
+                gtype = int(z[f"g{gi}_type"])
+                compare(got, ref, golden_tolerance(gtype, k))
+                if gtype == L.SNOW:
+                    check_snow_f_percentile(got["F"], ref["F"], k)
                 off += n
 
 
