@@ -14,7 +14,7 @@ using SurFn = void (*)(ParticleBuf, FusedArgs, SurArgs);
 // k_g2p2g<dim, mat, kFusedCfgs[ci], fixed_scene>; fixed_scene: one scene whose
 // parameters do not change during the run, passed in FusedArgs::scene
 FusedFn fused_fn(int dim, int mat, int ci, bool fixed_scene);
-// k_g2p2g_sur<kFusedCfgs[ci]> (3D jello)
-SurFn sur_fn(int ci);
+// k_g2p2g_sur with `cta` threads (64 or 128), fixed_scene (3D jello)
+SurFn sur_fn(int cta, bool fixed_scene);
 
 }  // namespace mpm

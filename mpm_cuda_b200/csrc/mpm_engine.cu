@@ -448,17 +448,22 @@ void Engine::set_config(int ci) {
     grid_dirty = true;  // chunk lists depend on the chunk size
 }
 
+// CTA size of the learned-stress kernel: 128 threads when the chunk holds a
+// multiple of 128 particles (its shared rows then allow 16 warps per SM),
+// else the chunk's 64; it takes chunk_particles() / that many rounds
+int Engine::sur_chunk() const { return chunk_particles() % 128 == 0 ? 128 : 64; }
+
 void Engine::sur_occupancy() {
     for (int mat = 0; mat < kMats; ++mat) {
         if (!sur_kernel(mat)) continue;
-        const int ch = kFusedCfgs[cfg].chunk;
+        const int ch = sur_chunk();
         int per_sm = 0;
         // the network rows live in dynamic shared memory; with the windows and
         // weights they can exceed the 48 KB a kernel gets without opting in
-        if (cudaFuncSetAttribute(sur_fn(cfg), cudaFuncAttributeMaxDynamicSharedMemorySize, sur_dyn_smem(ch)) !=
+        if (cudaFuncSetAttribute(sur_fn(ch, fixed_scene), cudaFuncAttributeMaxDynamicSharedMemorySize, sur_dyn_smem(ch)) !=
             cudaSuccess)
             cudaGetLastError();  // not fatal here: the occupancy query and the launch report it
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sur_fn(cfg), ch, sur_dyn_smem(ch)) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sur_fn(ch, fixed_scene), ch, sur_dyn_smem(ch)) !=
             cudaSuccess) {
             cudaGetLastError();
             per_sm = 1;
@@ -757,6 +762,13 @@ FusedArgs Engine::fused_args(int mat, bool bump) {
     A.rounds = kFusedCfgs[cfg].rounds;
     A.defer_vc = defer_vc_now() ? 1 : 0;
     A.scene = scenes_h[0];
+    // the material's only group, when it has one
+    int n_of_mat = 0;
+    A.one_group = 0;
+    A.group = GroupParams{};
+    for (const GroupParams& g : groups_h)
+        if (g.type == mat && ++n_of_mat == 1) A.group = g;
+    A.one_group = n_of_mat == 1 ? 1 : 0;
     return A;
 }
 
@@ -799,9 +811,13 @@ void Engine::enqueue_g2p2g(int parity) {
         bump = false;
         if (sur_kernel(mat)) {
             const SurArgs SA{&sur->weights->f, sur->meta, sur_counts};
-            const int ch = kFusedCfgs[cfg].chunk;
-            sur_fn(cfg)<<<sur_ctas[mat], ch, sur_dyn_smem(ch), stream>>>(buf(parity), A, SA);
-            note_launch("k_g2p2g_sur");
+            const int ch = sur_chunk();
+            FusedArgs As = A;
+            As.rounds = chunk_particles() / ch;
+            cudaLaunchAttribute attr;
+            const cudaLaunchConfig_t lc = pdl_config(sur_ctas[mat], ch, sur_dyn_smem(ch), stream, &attr);
+            const cudaError_t e = cudaLaunchKernelEx(&lc, sur_fn(ch, fixed_scene), buf(parity), As, SA);
+            note_launch_status("k_g2p2g_sur", e);
         } else {
             cudaLaunchAttribute attr;
             const cudaLaunchConfig_t lc = pdl_config(fused_ctas[mat], kFusedCfgs[cfg].chunk,
@@ -894,15 +910,8 @@ int Engine::canonical_order() {
     return take_launch_error();
 }
 
-// makes grid_mom hold the P2G of the current state (binned path): sorts the
-// particles into fresh chunks and scatters them straight to global memory
-// the fused kernels defer v and C unless a learned-stress kernel runs (it
-// reads back the v and C it stores)
-bool Engine::defer_vc_now() const {
-    for (int mat = 0; mat < kMats; ++mat)
-        if (mat_present[mat] && sur_kernel(mat)) return false;
-    return true;
-}
+// the fused kernels (plain and learned-stress) defer v and C
+bool Engine::defer_vc_now() const { return true; }
 
 // rebuilds the deferred v and C planes (k_recover_vc) before anything reads
 // them: the state download and upload, the first P2G of a state, the other
@@ -922,6 +931,8 @@ int Engine::recover_vc() {
     return MPM_OK;
 }
 
+// makes grid_mom hold the P2G of the current state (binned path): sorts the
+// particles into fresh chunks and scatters them straight to global memory
 int Engine::prologue() {
     {
         const int rc = recover_vc();

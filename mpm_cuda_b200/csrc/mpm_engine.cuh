@@ -166,6 +166,7 @@ struct Engine {
     // jello only: snow's exact stress reuses its plasticity decomposition
     bool sur_kernel(int mat) const { return sur && dim == 3 && mat == JELLO; }
     void sur_occupancy();
+    int sur_chunk() const;
     int sur_refresh();
     void enqueue_det_p2g();
     void enqueue_det_substep();

@@ -4,27 +4,19 @@
 
 namespace mpm {
 
-// the surrogate kernel of a fused-kernel configuration (same chunk and
-// launch-bound occupancy as its direct-scatter instantiation)
-template <int K>
+// The learned-stress kernel for a CTA size (64 or 128 threads; the engine
+// picks 128 when the chunk holds a multiple of 128 particles), with launch
+// bounds at the CTAs per SM its shared memory allows (velocity windows,
+// network weights, network and stash rows: 5 CTAs of 64, 4 of 128 threads),
+// so its registers are not capped below what that occupancy leaves them.
+template <int CHUNK, bool FIXED>
 static constexpr auto sur_kernel() {
-    return &k_g2p2g_sur<kFusedKernels[K].chunk, kFusedKernels[K].min_ctas>;
+    return &k_g2p2g_sur<CHUNK, CHUNK == 64 ? 5 : 4, FIXED>;
 }
 
-SurFn sur_fn(int ci) {
-    static_assert(kNumFusedKernels == 12, "update the dispatch table");
-    // the learned-stress kernel scatters directly: a segmented configuration
-    // runs it with the direct instantiation of its chunk
-    switch (direct_kernel_of(kFusedCfgs[ci].kernel)) {
-        case 0: return sur_kernel<0>();
-        case 1: return sur_kernel<1>();
-        case 2: return sur_kernel<2>();
-        case 3: return sur_kernel<3>();
-        case 4: return sur_kernel<4>();
-        case 5: return sur_kernel<5>();
-        case 6: return sur_kernel<6>();
-        default: return sur_kernel<7>();
-    }
+SurFn sur_fn(int cta, bool fixed_scene) {
+    if (cta == 64) return fixed_scene ? sur_kernel<64, true>() : sur_kernel<64, false>();
+    return fixed_scene ? sur_kernel<128, true>() : sur_kernel<128, false>();
 }
 
 }  // namespace mpm

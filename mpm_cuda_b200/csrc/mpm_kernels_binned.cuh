@@ -345,7 +345,19 @@ struct FusedArgs {
     // built with FIXED = true from their parameters (constant bank operands,
     // no loads) instead of from `scenes`
     SceneParams scene;
+    // one_group != 0: every particle of this launch's material belongs to
+    // `group`, which the FIXED kernels then take from their parameters instead
+    // of loading each particle's group index and group record
+    int one_group;
+    GroupParams group;
 };
+
+// the group record of particle i of a fused launch
+template <bool FIXED>
+__device__ __forceinline__ GroupParams particle_group(const FusedArgs& A, const ParticleBuf& pb, long long i) {
+    if (FIXED && A.one_group) return A.group;
+    return A.groups[pb.grp[i]];
+}
 
 // the scene of chunk's scene index si: from the kernel parameters when FIXED
 template <bool FIXED>
@@ -746,7 +758,7 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
                     G2PAcc<D> acc;
                     g2p_window<D>(st, o, w, sc, A, acc);
                     // loaded after the gather, its register peak
-                    const GroupParams g = A.groups[pb.grp[i]];
+                    const GroupParams g = particle_group<FIXED>(A, pb, i);
                     float F[D * D], Cn[D * D], v[D], aux;
                     ElasticSVD<D> esvd;  // snow: the plasticity step's decomposition, reused by the stress
                     err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux,

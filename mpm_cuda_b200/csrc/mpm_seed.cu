@@ -57,18 +57,26 @@ struct SeedParams {
     double blo[2], bhi[2];
 };
 
+// Every floating-point operation that decides which samples are kept is
+// rounded explicitly (no multiply-add contraction), so a CPU restatement with
+// the same operations reproduces the output bit for bit.
+__device__ __forceinline__ double dsub(double a, double b) { return __dadd_rn(a, -b); }
+__device__ __forceinline__ double dcross(double a, double b, double c, double d) {
+    return dsub(__dmul_rn(a, b), __dmul_rn(c, d));  // a b - c d
+}
+
 // 2D edge function with a top-left tie rule: a point on an edge belongs to
 // the triangle on one fixed side of it
 __device__ __forceinline__ bool edge_in(double ax, double ay, double bx, double by, double px, double py) {
-    const double e = (bx - ax) * (py - ay) - (by - ay) * (px - ax);
+    const double e = dcross(dsub(bx, ax), dsub(py, ay), dsub(by, ay), dsub(px, ax));
     if (e != 0.0) return e > 0.0;
     return (by > ay) || (by == ay && bx < ax);
 }
 
 __device__ bool inside_mesh(const SeedParams& P, const double* l) {
     if (!(l[0] >= P.blo[0] && l[0] < P.bhi[0] && l[1] >= P.blo[1] && l[1] < P.bhi[1])) return false;
-    const int bx = min(P.nbx - 1, (int)((l[0] - P.blo[0]) / (P.bhi[0] - P.blo[0]) * P.nbx));
-    const int by = min(P.nby - 1, (int)((l[1] - P.blo[1]) / (P.bhi[1] - P.blo[1]) * P.nby));
+    const int bx = min(P.nbx - 1, (int)__dmul_rn(__ddiv_rn(dsub(l[0], P.blo[0]), dsub(P.bhi[0], P.blo[0])), P.nbx));
+    const int by = min(P.nby - 1, (int)__dmul_rn(__ddiv_rn(dsub(l[1], P.blo[1]), dsub(P.bhi[1], P.blo[1])), P.nby));
     const int b = by * P.nbx + bx;
     int hits = 0;
     for (int k = P.bin_start[b]; k < P.bin_start[b + 1]; ++k) {
@@ -79,7 +87,7 @@ __device__ bool inside_mesh(const SeedParams& P, const double* l) {
         double ax = A[0], ay = A[1], bxx = B[0], byy = B[1], cx = Cc[0], cy = Cc[1];
         double az = A[2], bz = B[2], cz = Cc[2];
         // orient the projected triangle counter-clockwise
-        const double area = (bxx - ax) * (cy - ay) - (byy - ay) * (cx - ax);
+        const double area = dcross(dsub(bxx, ax), dsub(cy, ay), dsub(byy, ay), dsub(cx, ax));
         if (area == 0.0) continue;  // seen edge-on by the ray
         if (area < 0.0) {
             double tx = bxx, ty = byy, tz = bz;
@@ -91,9 +99,10 @@ __device__ bool inside_mesh(const SeedParams& P, const double* l) {
             continue;
         // height of the triangle's plane above the sample
         const double a2 = fabs(area);
-        const double wa = ((bxx - l[0]) * (cy - l[1]) - (byy - l[1]) * (cx - l[0])) / a2;
-        const double wb = ((cx - l[0]) * (ay - l[1]) - (cy - l[1]) * (ax - l[0])) / a2;
-        const double z = wa * az + wb * bz + (1.0 - wa - wb) * cz;
+        const double wa = __ddiv_rn(dcross(dsub(bxx, l[0]), dsub(cy, l[1]), dsub(byy, l[1]), dsub(cx, l[0])), a2);
+        const double wb = __ddiv_rn(dcross(dsub(cx, l[0]), dsub(ay, l[1]), dsub(cy, l[1]), dsub(ax, l[0])), a2);
+        const double z = __dadd_rn(__dadd_rn(__dmul_rn(wa, az), __dmul_rn(wb, bz)),
+                                   __dmul_rn(dsub(dsub(1.0, wa), wb), cz));
         if (z > l[2]) ++hits;
     }
     return (hits & 1) != 0;
@@ -114,17 +123,19 @@ __device__ bool sample(const SeedParams& P, long long cell, int ix, int iy, int 
         if ((double)f >= hi) f = nextafterf(f, -INFINITY);
         if ((double)f < lo) f = nextafterf(f, INFINITY);
         w[a] = f;
-        q[a] = ((double)w[a] - P.T[a]) / P.S[a];
+        q[a] = __ddiv_rn(dsub((double)w[a], P.T[a]), P.S[a]);
     }
     double l[3];
-    for (int a = 0; a < 3; ++a) l[a] = P.R[a] * q[0] + P.R[3 + a] * q[1] + P.R[6 + a] * q[2];  // R^T q
+    for (int a = 0; a < 3; ++a)  // R^T q
+        l[a] = __dadd_rn(__dadd_rn(__dmul_rn(P.R[a], q[0]), __dmul_rn(P.R[3 + a], q[1])), __dmul_rn(P.R[6 + a], q[2]));
     switch (P.shape) {
         case MPM_SHAPE_CUBE:
             return fabs(l[0]) <= 0.5 && fabs(l[1]) <= 0.5 && (P.dim == 2 || fabs(l[2]) <= 0.5);
         case MPM_SHAPE_SPHERE:
-            return l[0] * l[0] + l[1] * l[1] + (P.dim == 3 ? l[2] * l[2] : 0.0) <= 0.25;
+            return __dadd_rn(__dadd_rn(__dmul_rn(l[0], l[0]), __dmul_rn(l[1], l[1])),
+                             P.dim == 3 ? __dmul_rn(l[2], l[2]) : 0.0) <= 0.25;
         case MPM_SHAPE_CYLINDER:
-            return l[0] * l[0] + l[2] * l[2] <= 0.25 && fabs(l[1]) <= 0.5;
+            return __dadd_rn(__dmul_rn(l[0], l[0]), __dmul_rn(l[2], l[2])) <= 0.25 && fabs(l[1]) <= 0.5;
         default:
             return inside_mesh(P, l);
     }

@@ -61,6 +61,9 @@ def load():
         lib.orc_g2p.argtypes = [C.POINTER(OrcGrid), C.POINTER(OrcGroup), C.POINTER(OrcParticles), _DP, C.c_int]
         lib.orc_kirchhoff_fcr.argtypes = [C.c_int, _DP, C.c_double, C.c_double, _DP]
         lib.orc_polar_svd.argtypes = [C.c_int, _DP, _DP, _DP, _DP]
+        lib.orc_seed.argtypes = [C.c_int, _DP, _DP, _DP, C.POINTER(C.c_float), C.c_long, C.POINTER(C.c_int),
+                                 C.c_long, C.c_int, C.c_double, _DP, C.c_int, C.c_ulonglong,
+                                 C.POINTER(C.c_float), C.c_long, C.POINTER(C.c_long)]
         lib.orc_bspline.argtypes = [C.c_double]
         lib.orc_bspline.restype = C.c_double
         lib.orc_bspline_deriv.argtypes = [C.c_double]
@@ -200,3 +203,34 @@ def bspline(x: float) -> float:
 
 def bspline_deriv(x: float) -> float:
     return load().orc_bspline_deriv(x)
+
+
+SEED_SHAPES = {"cube": 0, "sphere": 1, "cylinder": 2, "mesh": 3}
+
+
+def seed_positions(shape: str, h: float, ppc: int, *, translation=(0.0, 0.0, 0.0), scale=(1.0, 1.0, 1.0),
+                   rot=None, origin=(0.0, 0.0, 0.0), dim: int = 3, seed_value: int = 1234, vertices=None,
+                   triangles=None) -> np.ndarray:
+    """The CPU restatement of the GPU seeding (orc_seed): positions (n, dim)
+    float32 in cell order, bit for bit what mpm_seed returns."""
+    lib = load()
+    R = np.ascontiguousarray(np.eye(3) if rot is None else rot, np.float64).ravel()
+    S = np.ascontiguousarray(list(scale) + [1.0] * (3 - len(scale)), np.float64)[:3]
+    T = np.ascontiguousarray(list(translation) + [0.0] * (3 - len(translation)), np.float64)[:3]
+    O = np.ascontiguousarray(list(origin) + [0.0] * (3 - len(origin)), np.float64)[:3]
+    v = t = None
+    nv = nt = 0
+    if shape == "mesh":
+        v = np.ascontiguousarray(vertices, np.float32)
+        t = np.ascontiguousarray(triangles, np.int32)
+        nv, nt = v.shape[0], t.shape[0]
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
+    ip = t.ctypes.data_as(C.POINTER(C.c_int)) if t is not None else None
+    n = C.c_long()
+    args = (SEED_SHAPES[shape], _dp(R), _dp(S), _dp(T), fp(v), nv, ip, nt, dim, h, _dp(O), ppc, seed_value)
+    if lib.orc_seed(*args, None, 0, C.byref(n)) != 0:
+        raise ValueError("orc_seed: bad argument")
+    out = np.empty((n.value, dim), np.float32)
+    if n.value and lib.orc_seed(*args, fp(out), out.size, C.byref(n)) != 0:
+        raise ValueError("orc_seed failed")
+    return out

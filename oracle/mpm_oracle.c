@@ -21,6 +21,7 @@
 #include "mpm_oracle.h"
 
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
 #include <omp.h>
@@ -461,4 +462,222 @@ int orc_substep(const orc_grid *g, const orc_group *groups, orc_particles *p,
     err |= orc_grid_update(g, grid_mass, grid_mom);
     err |= orc_g2p(g, groups, p, grid_mom, nthreads);
     return err;
+}
+
+
+/* ------------------------------------------------------------------ seeding
+ * Restatement of mpm_seed (mpm_cuda_b200/csrc/mpm_seed.cu), operation for
+ * operation; this file is compiled with -ffp-contract=off. */
+
+/* splitmix64 finaliser (Steele, Lea, Flood 2014) */
+static unsigned long long seed_mix(unsigned long long z) {
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+typedef struct {
+    int shape, dim, ppc;
+    double R[9], S[3], T[3], h, origin[3];
+    int i0[3], ni[3];
+    unsigned long long seed;
+    const float *vert;
+    const int *tri, *bin_start, *bin_tri;
+    int nbx, nby;
+    double blo[2], bhi[2];
+} seed_params;
+
+static double dcross(double a, double b, double c, double d) { return a * b - c * d; }
+
+static int edge_in(double ax, double ay, double bx, double by, double px, double py) {
+    const double e = dcross(bx - ax, py - ay, by - ay, px - ax);
+    if (e != 0.0) return e > 0.0;
+    return (by > ay) || (by == ay && bx < ax);
+}
+
+static int inside_mesh(const seed_params *P, const double *l) {
+    if (!(l[0] >= P->blo[0] && l[0] < P->bhi[0] && l[1] >= P->blo[1] && l[1] < P->bhi[1])) return 0;
+    int bx = (int)((l[0] - P->blo[0]) / (P->bhi[0] - P->blo[0]) * P->nbx);
+    int by = (int)((l[1] - P->blo[1]) / (P->bhi[1] - P->blo[1]) * P->nby);
+    if (bx > P->nbx - 1) bx = P->nbx - 1;
+    if (by > P->nby - 1) by = P->nby - 1;
+    const int b = by * P->nbx + bx;
+    int hits = 0;
+    for (int k = P->bin_start[b]; k < P->bin_start[b + 1]; ++k) {
+        const int t = P->bin_tri[k];
+        const float *A = P->vert + 3 * P->tri[3 * t], *B = P->vert + 3 * P->tri[3 * t + 1],
+                    *Cc = P->vert + 3 * P->tri[3 * t + 2];
+        double ax = A[0], ay = A[1], bxx = B[0], byy = B[1], cx = Cc[0], cy = Cc[1];
+        double az = A[2], bz = B[2], cz = Cc[2];
+        const double area = dcross(bxx - ax, cy - ay, byy - ay, cx - ax);
+        if (area == 0.0) continue;
+        if (area < 0.0) {
+            double tx = bxx, ty = byy, tz = bz;
+            bxx = cx; byy = cy; bz = cz;
+            cx = tx; cy = ty; cz = tz;
+        }
+        if (!edge_in(ax, ay, bxx, byy, l[0], l[1]) || !edge_in(bxx, byy, cx, cy, l[0], l[1]) ||
+            !edge_in(cx, cy, ax, ay, l[0], l[1]))
+            continue;
+        const double a2 = fabs(area);
+        const double wa = dcross(bxx - l[0], cy - l[1], byy - l[1], cx - l[0]) / a2;
+        const double wb = dcross(cx - l[0], ay - l[1], cy - l[1], ax - l[0]) / a2;
+        const double z = (wa * az + wb * bz) + ((1.0 - wa) - wb) * cz;
+        if (z > l[2]) ++hits;
+    }
+    return hits & 1;
+}
+
+/* sample k of lattice cell (ix, iy, iz), linear cell index `cell` */
+static int seed_sample(const seed_params *P, long long cell, int ix, int iy, int iz, int k, float *w) {
+    const unsigned long long base = seed_mix(P->seed ^ seed_mix((unsigned long long)cell * 64ull + (unsigned)k));
+    const int ic[3] = {ix, iy, iz};
+    double q[3] = {0.0, 0.0, 0.0};
+    for (int a = 0; a < P->dim; ++a) {
+        const double u = (double)(seed_mix(base + (unsigned long long)a) >> 11) * (1.0 / 9007199254740992.0);
+        const double lo = P->origin[a] + (double)ic[a] * P->h;
+        const double hi = P->origin[a] + ((double)ic[a] + 1.0) * P->h;
+        float f = (float)(P->origin[a] + ((double)ic[a] + u) * P->h);
+        if ((double)f >= hi) f = nextafterf(f, -INFINITY);
+        if ((double)f < lo) f = nextafterf(f, INFINITY);
+        w[a] = f;
+        q[a] = ((double)w[a] - P->T[a]) / P->S[a];
+    }
+    double l[3];
+    for (int a = 0; a < 3; ++a) l[a] = (P->R[a] * q[0] + P->R[3 + a] * q[1]) + P->R[6 + a] * q[2];
+    switch (P->shape) {
+        case 0:
+            return fabs(l[0]) <= 0.5 && fabs(l[1]) <= 0.5 && (P->dim == 2 || fabs(l[2]) <= 0.5);
+        case 1:
+            return (l[0] * l[0] + l[1] * l[1]) + (P->dim == 3 ? l[2] * l[2] : 0.0) <= 0.25;
+        case 2:
+            return l[0] * l[0] + l[2] * l[2] <= 0.25 && fabs(l[1]) <= 0.5;
+        default:
+            return inside_mesh(P, l);
+    }
+}
+
+int orc_seed(int shape, const double *rotation, const double *scale, const double *translation,
+             const float *vertices, long n_vertices, const int *triangles, long n_triangles, int dim,
+             double h, const double *origin, int ppc, unsigned long long seed, float *out, long cap,
+             long *n_out) {
+    if (!n_out || !(h > 0.0) || ppc < 1 || ppc > 64 || (dim != 2 && dim != 3) || shape < 0 || shape > 3) return -1;
+    seed_params P;
+    memset(&P, 0, sizeof(P));
+    P.shape = shape;
+    P.dim = dim;
+    P.ppc = ppc;
+    P.h = h;
+    P.seed = seed;
+    for (int a = 0; a < 9; ++a) P.R[a] = rotation[a];
+    for (int a = 0; a < 3; ++a) {
+        P.S[a] = scale[a];
+        P.T[a] = translation[a];
+        P.origin[a] = origin ? origin[a] : 0.0;
+    }
+    double llo[3] = {-0.5, -0.5, -0.5}, lhi[3] = {0.5, 0.5, 0.5};
+    int *bin_start = NULL, *bin_tri = NULL;
+    if (shape == 3) {
+        if (dim != 3 || !vertices || !triangles || n_vertices <= 0 || n_triangles <= 0) return -1;
+        for (int a = 0; a < 3; ++a) {
+            llo[a] = 1e300;
+            lhi[a] = -1e300;
+        }
+        for (long v = 0; v < n_vertices; ++v)
+            for (int a = 0; a < 3; ++a) {
+                llo[a] = fmin(llo[a], (double)vertices[3 * v + a]);
+                lhi[a] = fmax(lhi[a], (double)vertices[3 * v + a]);
+            }
+        int nb = (int)sqrt((double)n_triangles);
+        if (nb > 256) nb = 256;
+        if (nb < 1) nb = 1;
+        P.nbx = P.nby = nb;
+        const double pad = 1e-9 * fmax(1.0, fmax(lhi[0] - llo[0], lhi[1] - llo[1]));
+        P.blo[0] = llo[0] - pad;
+        P.blo[1] = llo[1] - pad;
+        P.bhi[0] = lhi[0] + pad;
+        P.bhi[1] = lhi[1] + pad;
+        /* CSR triangle lists of the xy bins, triangles ascending in each bin */
+        int *counts = calloc((size_t)nb * nb + 1, sizeof(int));
+        int (*span)[4] = malloc((size_t)n_triangles * sizeof(*span));
+        for (long t = 0; t < n_triangles; ++t) {
+            double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300;
+            for (int c = 0; c < 3; ++c) {
+                const float *p = vertices + 3 * triangles[3 * t + c];
+                x0 = fmin(x0, (double)p[0]);
+                x1 = fmax(x1, (double)p[0]);
+                y0 = fmin(y0, (double)p[1]);
+                y1 = fmax(y1, (double)p[1]);
+            }
+            const double ev[4] = {x0, x1, y0, y1};
+            for (int e = 0; e < 4; ++e) {
+                const int ax = e / 2;
+                int bi = (int)((ev[e] - P.blo[ax]) / (P.bhi[ax] - P.blo[ax]) * nb);
+                span[t][e] = bi < 0 ? 0 : (bi > nb - 1 ? nb - 1 : bi);
+            }
+            for (int by = span[t][2]; by <= span[t][3]; ++by)
+                for (int bx = span[t][0]; bx <= span[t][1]; ++bx) counts[by * nb + bx + 1]++;
+        }
+        bin_start = malloc(((size_t)nb * nb + 1) * sizeof(int));
+        bin_start[0] = 0;
+        for (int b = 0; b < nb * nb; ++b) bin_start[b + 1] = bin_start[b] + counts[b + 1];
+        bin_tri = malloc((size_t)(bin_start[nb * nb] > 0 ? bin_start[nb * nb] : 1) * sizeof(int));
+        int *fill = calloc((size_t)nb * nb, sizeof(int));
+        for (long t = 0; t < n_triangles; ++t)
+            for (int by = span[t][2]; by <= span[t][3]; ++by)
+                for (int bx = span[t][0]; bx <= span[t][1]; ++bx) {
+                    const int b = by * nb + bx;
+                    bin_tri[bin_start[b] + fill[b]++] = (int)t;
+                }
+        free(fill);
+        free(span);
+        free(counts);
+        P.vert = vertices;
+        P.tri = triangles;
+        P.bin_start = bin_start;
+        P.bin_tri = bin_tri;
+    }
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int c = 0; c < 8; ++c) {
+        const double p[3] = {(c & 1) ? lhi[0] : llo[0], (c & 2) ? lhi[1] : llo[1], (c & 4) ? lhi[2] : llo[2]};
+        for (int a = 0; a < 3; ++a) {
+            const double w = P.T[a] + P.S[a] * ((P.R[a * 3] * p[0] + P.R[a * 3 + 1] * p[1]) + P.R[a * 3 + 2] * p[2]);
+            lo[a] = fmin(lo[a], w);
+            hi[a] = fmax(hi[a], w);
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        if (a >= dim) {
+            P.i0[a] = 0;
+            P.ni[a] = 1;
+            continue;
+        }
+        const double i0 = floor((lo[a] - P.origin[a]) / h), i1 = floor((hi[a] - P.origin[a]) / h) + 1.0;
+        P.i0[a] = (int)i0;
+        P.ni[a] = (int)(i1 - i0);
+    }
+    long n = 0;
+    int rc = 0;
+    float w[3];
+    for (int ix = 0; ix < P.ni[0]; ++ix)
+        for (int iy = 0; iy < P.ni[1]; ++iy)
+            for (int iz = 0; iz < P.ni[2]; ++iz) {
+                const long long cell = ((long long)ix * P.ni[1] + iy) * P.ni[2] + iz;
+                for (int k = 0; k < ppc; ++k)
+                    if (seed_sample(&P, cell, P.i0[0] + ix, P.i0[1] + iy, P.i0[2] + iz, k, w)) {
+                        if (out) {
+                            if ((n + 1) * dim > cap) {
+                                rc = -1;
+                                continue;
+                            }
+                            for (int a = 0; a < dim; ++a) out[n * dim + a] = w[a];
+                        }
+                        ++n;
+                    }
+            }
+    free(bin_start);
+    free(bin_tri);
+    *n_out = n;
+    return rc;
 }

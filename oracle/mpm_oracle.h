@@ -114,6 +114,20 @@ void orc_polar_svd(int dim, const double *F, double *U, double *s, double *V);
 double orc_bspline(double x);
 double orc_bspline_deriv(double x);
 
+/* CPU restatement of the project's particle seeding (mpm_seed in
+ * mpm_cuda_b200/csrc/mpm_seed.cu, which replaces the reference's rand()
+ * jitter and point-in-mesh loop, MPMSimulator.cpp:198-257): the same
+ * splitmix64 jitter per (seed, lattice cell, sample), the same inside tests
+ * and the same cell order, every floating-point operation in the same order
+ * without contraction, so the positions agree bit for bit.  shape: 0 cube,
+ * 1 sphere, 2 cylinder, 3 triangle mesh.  Writes up to cap floats to out
+ * (n * dim used) and the particle count to *n_out; returns 0, or -1 on a bad
+ * argument or a count above cap / dim. */
+int orc_seed(int shape, const double *rotation, const double *scale, const double *translation,
+             const float *vertices, long n_vertices, const int *triangles, long n_triangles, int dim,
+             double h, const double *origin, int ppc, unsigned long long seed, float *out, long cap,
+             long *n_out);
+
 #ifdef __cplusplus
 }
 #endif

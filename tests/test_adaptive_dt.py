@@ -67,3 +67,32 @@ def test_adaptive_needs_the_binned_path(gpu):
         with pytest.raises(L.MPMError) as e:
             sim.set_p2g_mode(L.P2G_DETERMINISTIC)
         assert e.value.code == L.ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("d", [2, 3])
+def test_the_chosen_dt_sequence_replays_through_the_fp64_oracle(gpu, d):
+    """The dt the device chose for every substep (read between substeps),
+    fed to the FP64 oracle substep by substep, reproduces the state: the
+    adaptive path differs from a fixed-dt run only in its dt sequence.  The
+    scene is a blob with perturbed v, C and F of a stiff, light jello, so the
+    wave speed binds dt below the scene's dt and the particles' speeds move it."""
+    from mpm_cuda_b200.sim import Scene
+    from helpers import compare, group_from_arrays, oracle_for
+    mat = S.jello(E=5e4, nu=0.3, rho=1.0)
+    h, n_grid = 1.0 / 32, 32
+    x, v, C_, F, aux = S.perturbed_blob(d, mat, n_grid=n_grid, h=h, ppc=2, radius_cells=5.0, seed=31,
+                                        center=np.full(d, 0.5))
+    sc = Scene(dim=d, n=(n_grid,) * d, h=h, dt=1e-4, groups=[group_from_arrays(mat, h, 2, x, v, C_, F, aux)],
+               bc_type=L.BC_SLIP, bc_lo=3, bc_hi=3, gravity=(0.0, -9.8, 0.0)[:d] if d == 3 else (0.0, -9.8))
+    orc = oracle_for(sc)
+    dts = []
+    with Simulation([sc], adaptive_dt=True, cfl=0.5, rebin_interval=4) as sim:
+        for _ in range(24):
+            dts.append(sim.scene_time(0)[1])
+            assert sim.step_status(1) == L.OK
+        got = sim.get_state(0)
+    assert len(set(dts)) > 1 and max(dts) < 1e-4, dts  # the bound binds and varies
+    for dt in dts:
+        orc.grid.dt = dt
+        assert orc.step(1) == 0
+    compare(got, orc.state(), {"x": 1e-5, "v": 2e-3, "C": 2e-3, "F": 1e-4, "aux": 1e-4})

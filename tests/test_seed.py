@@ -1,7 +1,8 @@
 """Particle seeding on the GPU (mpm_seed): counts follow the object's volume,
 every sample lies inside the object and inside its lattice cell, output is
-deterministic for a seed, and a triangle mesh of a shape seeds like the
-analytic shape."""
+deterministic for a seed, a triangle mesh of a shape seeds like the analytic
+shape, and the positions equal the CPU restatement's (oracle.cpu.seed_positions)
+bit for bit."""
 import ctypes as C
 
 import numpy as np
@@ -104,3 +105,56 @@ def test_2d_square(gpu):
     assert p.shape[1] == 2
     assert np.all(np.abs(p - np.array([0.5, 0.6], np.float32)) <= 0.1 + 1e-6)
     assert abs(len(p) - 0.04 * 128 ** 2 * 4) < 0.01 * 0.04 * 128 ** 2 * 4
+
+
+# ------------------------------------------------- against the CPU restatement
+
+def _cases():
+    from mpm_cuda_b200.seed import rotation
+    R = rotation((1.0, 2.0, 0.5), 30.0)
+    v, t = cube_mesh()
+    tv = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], np.float32) - 0.25
+    tt = np.array([[0, 2, 1], [0, 1, 3], [0, 3, 2], [1, 2, 3]], np.int32)
+    return [
+        ("cube", dict(h=1.0 / 128, ppc=8, translation=(0.5, 0.6, 0.5), scale=(0.3, 0.2, 0.25), rot=R, seed_value=7)),
+        ("sphere", dict(h=1.0 / 100, ppc=8, translation=(0.45, 0.5, 0.55), scale=(0.3, 0.3, 0.3), rot=R,
+                        seed_value=9, origin=(0.01, -0.02, 0.0))),
+        ("cylinder", dict(h=1.0 / 96, ppc=4, translation=(0.5, 0.5, 0.5), scale=(0.2, 0.4, 0.2), rot=R, seed_value=3)),
+        ("mesh", dict(h=1.0 / 96, ppc=4, translation=(0.5, 0.5, 0.5), scale=(0.4, 0.3, 0.35),
+                      rot=rotation((0.3, 1.0, 0.2), 17.0), seed_value=3, vertices=v, triangles=t)),
+        ("mesh", dict(h=1.0 / 128, ppc=8, translation=(0.5, 0.5, 0.5), scale=(0.5, 0.5, 0.5), seed_value=5,
+                      vertices=tv, triangles=tt)),
+        ("cube", dict(h=1.0 / 128, ppc=4, translation=(0.5, 0.6), scale=(0.2, 0.2, 1.0), dim=2, seed_value=11)),
+    ]
+
+
+def test_restatement_counts_and_containment():
+    """The CPU restatement alone: counts follow the volume, samples lie in
+    the object and in their lattice cell, cell order."""
+    from oracle import cpu as ocpu
+    for shape, kw in _cases():
+        p = ocpu.seed_positions(shape, **kw).astype(np.float64)
+        d = kw.get("dim", 3)
+        h, ppc = kw["h"], kw["ppc"]
+        S = np.asarray(kw["scale"], np.float64)[:d]
+        vol = {"cube": 1.0, "sphere": np.pi / 6, "cylinder": np.pi / 4}.get(shape)
+        if vol is None:  # meshes: the unit cube or the tetrahedron of volume 1/6
+            vol = 1.0 if len(kw["vertices"]) == 8 else 1.0 / 6
+        expect = vol * np.prod(S) / h ** d * ppc
+        assert abs(len(p) - expect) < 0.015 * expect, (shape, len(p), expect)
+        org = np.asarray(kw.get("origin", (0.0, 0.0, 0.0)), np.float64)[:d]
+        cell = np.floor((p - org) / h).astype(np.int64)
+        lin = cell[:, 0] * (1 << 40) + cell[:, 1] * (1 << 20) + (cell[:, 2] if d == 3 else 0)
+        assert np.all(np.diff(lin) >= 0), shape
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", range(6))
+def test_gpu_seeding_is_bit_identical_to_the_restatement(gpu, case):
+    from mpm_cuda_b200.seed import seed
+    from oracle import cpu as ocpu
+    shape, kw = _cases()[case]
+    got = seed(shape, **kw)
+    want = ocpu.seed_positions(shape, **kw)
+    assert len(got) > 1000
+    assert got.shape == want.shape and np.array_equal(got.view(np.uint32), want.view(np.uint32)), shape

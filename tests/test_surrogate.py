@@ -219,6 +219,53 @@ def test_fused_surrogate_drift_vs_plain(trained, harvested, gpu):
 
 
 @pytest.mark.gpu
+def test_c3_scene_stress_error_and_drift(surrogate_cls, gpu):
+    """The 256^3 jello scene (0.245 cube, ~2.0M particles, v = (0, -2, 0)):
+    trained on deformation gradients harvested after the impact (substeps
+    1600-3000 of a plain run), the network's held-out stress error is <= 1 %
+    and, from the state at substep 1400, 1000 substeps through the impact
+    drift <= 0.5 % of the cube edge (mean position distance) from the plain
+    path."""
+    from mpm_cuda_b200 import _lib as L
+    from mpm_cuda_b200 import scenes as S
+    from mpm_cuda_b200.sim import Simulation
+    from mpm_cuda_b200.train_surrogate import stress_error
+    edge = 0.245
+    snaps = []
+    with Simulation([S.c3_jello3d(edge=edge)]) as sim:
+        sim.step(1400)
+        before = sim.get_state(0)
+        for _ in range(8):
+            sim.step(200)
+            snaps.append(sim.get_state(0)["F"])
+        sim.step(350)
+        held = sim.get_state(0)["F"]
+    rng = np.random.default_rng(0)
+    train = np.concatenate(snaps)
+    train = train[rng.choice(len(train), 2_000_000, replace=False)]
+    sur = surrogate_cls(seed=11)
+    sur.train(train)
+    err, accepted = stress_error(sur, held[rng.choice(len(held), 500_000, replace=False)], 0.3)
+    assert err <= 1e-2 and accepted > 0.95, (err, accepted)
+    sc = S.c3_jello3d(edge=edge)
+    with Simulation([sc]) as plain, Simulation([sc]) as sim:
+        for s in (plain, sim):
+            s.set_state(0, before["x"], before["v"], before["C"], before["F"], before["aux"])
+        sim.set_stress_mode(L.STRESS_SURROGATE, sur)
+        plain.step(1000)
+        sim.step(1000)
+        assert sim.device_errors() == 0
+        n_net, n_fb = sim.stress_stats()
+        xp, xs = plain.get_state(0)["x"], sim.get_state(0)["x"]
+    sur.close()
+    drift = float(np.mean(np.linalg.norm(xs.astype(np.float64) - xp, axis=1))) / edge
+    share = n_net / (n_net + n_fb)
+    print(f"c3: held-out stress error {err:.4f}, network share {share:.4f}, mean drift {drift:.3e} of the edge")
+    assert share > 0.95
+    assert drift <= 5e-3
+
+
+@pytest.mark.gpu
 def test_snow_keeps_the_plain_stress(trained, gpu):
     # snow's exact stress reuses its plasticity decomposition, so surrogate
     # mode leaves it on the plain kernel: no particle goes through the network
