@@ -425,12 +425,9 @@ def run_ours(args, rank, world, local_rank, dist):
 
 # ----------------------------------------------------------- reference arm
 
-def run_reference(args):
+def _ref_sim(sc):
+    """The reference simulator holding one scene's particles (its constants)."""
     from oracle import ref as R
-    if not R.available():
-        return {"impl": "reference", "unavailable": "oracle/_ref/libmpm_ref.so was not built (needs the reference tree)"}
-    scenes, desc = build_workload("c1" if args.workload not in ("c1", "c3", "c2") else args.workload, 0, 1)
-    sc = scenes[0]
     sim = R.RefSim(sc.h, sc.dt, sc.n)
     for g in sc.groups:
         m = g.material
@@ -442,23 +439,67 @@ def run_reference(args):
         J = np.ones(n) if m.type == 2 else None
         sim.add_group(m.type, m.E if m.type != 2 else 1e4, m.nu if m.type != 2 else 0.2, m.rho, g.p_mass,
                       g.p_vol, x, v, F, Fp=Fp, J=J, C_=np.zeros((n, 3, 3)))
+    return sim
+
+
+def run_reference(args):
+    """The reference's own implementation of the substep on the workload: its
+    CUDA step() (oracle/_ref) for the 3D scenes -- the 64 batched scenes as 64
+    reference simulators stepped one after the other, as the reference runs one
+    scene per simulator -- and, for the 2D scene, whose reference is a Taichi
+    script that is not installed on either machine, the CPU port on all host
+    cores."""
+    from oracle import ref as R
+    scenes, desc = build_workload(args.workload, 0, 1)
     steps = min(args.steps, 200)
     warm = min(args.warmup, 20)
-    sim.step(warm)
-    repeats = [sim.time_steps(steps) for _ in range(REF_REPEATS)]
+    base = {"impl": "reference", "metric": METRIC, "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "data": "synthetic (seeded)"}
+    if scenes[0].dim == 2:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from helpers import oracle_for
+        sc = scenes[0]
+        orc = oracle_for(sc)
+        cores = os.cpu_count() or 1
+        orc.step(warm, threads=cores)
+        t0 = time.perf_counter()
+        orc.step(steps, threads=cores)
+        dt = time.perf_counter() - t0
+        value = sc.n_particles * steps / dt
+        sample = (f"{steps} substeps of {desc} after {warm} warm-up; the reference's 2D path is the Taichi script "
+                  "MPMJello.py (not installed here or on the GPU box), so its C restatement (FP64, OpenMP) runs")
+        return {**base, "value": value, "steps": steps, "warmup": warm, "ms_per_step": dt * 1e3 / steps,
+                "dtype": "f64", "config": {"workload": desc, "particles_per_gpu": sc.n_particles},
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not R.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libmpm_ref.so was not built (needs the reference tree)"}
+    n = sum(sc.n_particles for sc in scenes)
+    if len(scenes) == 1:
+        sim = _ref_sim(scenes[0])
+        sim.step(warm)
+        repeats = [sim.time_steps(steps) for _ in range(REF_REPEATS)]
+        sim.close()
+        how = f"median of {REF_REPEATS} timings of {steps} consecutive substeps"
+    else:
+        # one reference simulator per scene; each repeat times `steps` substeps
+        # of every scene, scene after scene
+        sims = [_ref_sim(sc) for sc in scenes]
+        for sim in sims:
+            sim.step(warm)
+        repeats = [sum(sim.time_steps(steps) for sim in sims) for _ in range(REF_REPEATS)]
+        for sim in sims:
+            sim.close()
+        how = (f"{len(scenes)} reference simulators, one per scene; median of {REF_REPEATS} timings of {steps} "
+               "substeps of every scene")
     ms = statistics.median(repeats)
-    sim.close()
-    n = sc.n_particles
     value = n * steps / (ms * 1e-3)
-    return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps,
-            "warmup": warm, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+    return {**base, "value": value, "steps": steps, "warmup": warm, "ms_per_step": ms / steps, "dtype": "f64",
             "config": {"workload": desc, "particles_per_gpu": n,
                        "repeats_ms_per_step": [round(r / steps, 4) for r in repeats],
                        "note": "reference MPMSimulator::step() (MPMCUDA.cu:793-925) built unmodified for sm_100a; "
                                "its stock path: FP64 state, 3 device syncs and a D2H position copy per substep; "
-                               "its hard-coded 10h walls and constants; median of "
-                               f"{REF_REPEATS} timings of {steps} consecutive substeps"},
+                               f"its hard-coded 10h walls and constants; {how}"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                              "sample": f"{steps} substeps of {desc}; the reference implementation of this path "
                                        "is CUDA, so it runs on the B200 driven by one host thread"},
