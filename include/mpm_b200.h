@@ -87,7 +87,9 @@ enum mpm_device_error {
     MPM_DEVERR_NONFINITE = 2,   /* NaN or Inf in particle state */
     MPM_DEVERR_DET = 4,         /* det F <= 0, det Fp <= 0 or J <= 0 */
     MPM_DEVERR_BINNING = 8,     /* internal: particle binning counts disagreed */
-    MPM_DEVERR_TIMEOUT = 16     /* a bounded device-side wait gave up */
+    MPM_DEVERR_TIMEOUT = 16,    /* a bounded device-side wait gave up */
+    MPM_DEVERR_POOL = 32        /* the paged grid's pool ran out of blocks
+                                   (mpm_options.grid_pool_blocks) */
 };
 
 typedef struct mpm_material_desc {
@@ -162,6 +164,18 @@ typedef struct mpm_options {
                            computes a dt factor it never applies,
                            MPMCUDA.cu:915-920).  Default 0 (fixed dt). */
     float cfl;          /* CFL number of adaptive dt, (0, 1]; default 0.5 */
+    int grid_pool_blocks; /* MPM_P2G_ATOMIC only.  0 (default): each scene's grid
+                           is allocated densely (the reference allocates its
+                           grid densely, MPMSimulator.cpp:122-146).  > 0: the
+                           grid is paged: one pool of this many 64-node blocks
+                           shared by all scenes, pages
+                           assigned on the device to the blocks particles
+                           touch and their neighbours and returned when nothing
+                           is active near them; a step that needs more blocks
+                           than the pool holds sets MPM_DEVERR_POOL.  Each
+                           pool block costs 2 KB of grid (momentum and
+                           velocity) plus 256 B per material of binning
+                           counters. */
 } mpm_options;
 
 typedef struct mpm_handle mpm_handle;
@@ -329,6 +343,13 @@ int mpm_autotune(mpm_handle *h, int n_substeps, int *chosen, float *ms_per_subst
  * scatters that left their block's shared-memory tile (served from global
  * memory) since creation; *rebins counts re-binnings. */
 int mpm_get_bin_stats(mpm_handle *h, int64_t *fallbacks, int64_t *rebins);
+
+/* Paged grid (mpm_options.grid_pool_blocks > 0): *capacity = the pool's
+ * 64-node blocks, *in_use = the blocks holding a page after the substeps
+ * enqueued so far (waits for the stream).  A dense grid reports its block
+ * count for both.  The reference allocates its grid densely
+ * (MPMSimulator.cpp:122-146) and has no counterpart. */
+int mpm_get_grid_pool(mpm_handle *h, int64_t *capacity, int64_t *in_use);
 
 /* Substeps without any device allocation, for callers that cannot allocate:
  * plug-in hosts with a fixed device memory budget, loops that forbid

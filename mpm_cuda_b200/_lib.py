@@ -21,7 +21,7 @@ BC_STICKY, BC_SLIP, BC_SEPARATE = 0, 1, 2
 P2G_ATOMIC, P2G_DETERMINISTIC, P2G_DIRECT = 0, 1, 2
 STRESS_PLAIN, STRESS_SURROGATE = 0, 1
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_SIM, ERR_IO = 0, -1, -2, -3, -4, -5, -6
-DEVERR_OUT_OF_GRID, DEVERR_NONFINITE, DEVERR_DET, DEVERR_BINNING, DEVERR_TIMEOUT = 1, 2, 4, 8, 16
+DEVERR_OUT_OF_GRID, DEVERR_NONFINITE, DEVERR_DET, DEVERR_BINNING, DEVERR_TIMEOUT, DEVERR_POOL = 1, 2, 4, 8, 16, 32
 
 _FP = C.POINTER(C.c_float)
 
@@ -48,7 +48,8 @@ class SceneDesc(C.Structure):
 class Options(C.Structure):
     _fields_ = [("p2g_mode", C.c_int), ("stress_mode", C.c_int), ("use_graph", C.c_int),
                 ("block_threads", C.c_int), ("device", C.c_int), ("rebin_interval", C.c_int),
-                ("kernel_config", C.c_int), ("adaptive_dt", C.c_int), ("cfl", C.c_float)]
+                ("kernel_config", C.c_int), ("adaptive_dt", C.c_int), ("cfl", C.c_float),
+                ("grid_pool_blocks", C.c_int)]
 
 
 SHAPE_CUBE, SHAPE_SPHERE, SHAPE_CYLINDER, SHAPE_MESH = 0, 1, 2, 3
@@ -95,6 +96,7 @@ EXPORTS = {
     "mpm_profile_stages": (C.c_int, [C.c_void_p, C.c_int, _FP, C.c_int, C.POINTER(C.c_int)]),
     "mpm_count_active_nodes": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]),
     "mpm_get_bin_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "mpm_get_grid_pool": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "mpm_num_kernel_configs": (C.c_int, []),
     "mpm_kernel_config_info": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "mpm_kernel_config_scatter": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),

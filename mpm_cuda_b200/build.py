@@ -21,8 +21,8 @@ BUILD_DIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "--expt-relaxed-constexpr", "-I", CSRC, "-I", INCLUDE]
-CU_SOURCES = ["mpm_abi.cu", "mpm_engine.cu", "mpm_fused_plain.cu", "mpm_fused_fixed.cu", "mpm_fused_sur.cu", "mpm_noalloc.cu",
-              "mpm_surrogate.cu", "mpm_seed.cu"]
+CU_SOURCES = ["mpm_abi.cu", "mpm_engine.cu", "mpm_fused_plain.cu", "mpm_fused_fixed.cu", "mpm_fused_paged.cu",
+              "mpm_fused_paged_fixed.cu", "mpm_fused_sur.cu", "mpm_noalloc.cu", "mpm_surrogate.cu", "mpm_seed.cu"]
 CPP_SOURCES = ["bgeo.cpp"]
 
 

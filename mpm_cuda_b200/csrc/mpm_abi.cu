@@ -60,6 +60,7 @@ void mpm_default_options(mpm_options* opt) {
     opt->device = 0;
     opt->rebin_interval = 0;
     opt->kernel_config = -1;
+    opt->grid_pool_blocks = 0;
 }
 
 int mpm_create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options* opt,
@@ -196,6 +197,11 @@ int mpm_get_bin_stats(mpm_handle* h, int64_t* fallbacks, int64_t* rebins) {
     return h->eng.bin_stats(fallbacks, rebins);
 }
 
+int mpm_get_grid_pool(mpm_handle* h, int64_t* capacity, int64_t* in_use) {
+    if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_get_grid_pool: NULL handle");
+    return h->eng.grid_pool(capacity, in_use);
+}
+
 int mpm_num_kernel_configs(void) { return mpm::kNumFusedCfgs; }
 
 int mpm_kernel_config_info(int config, int* chunk, int* min_ctas, int* rounds) {
@@ -225,6 +231,8 @@ int mpm_set_kernel_config(mpm_handle* h, int config) {
     if (!h) return fail(nullptr, MPM_ERR_INVALID, "mpm_set_kernel_config: NULL handle");
     if (config < 0 || config >= mpm::kNumFusedCfgs)
         return fail(h, MPM_ERR_INVALID, "mpm_set_kernel_config: config %d out of range", config);
+    if (h->eng.paged && mpm::kFusedCfgs[config].scatter != mpm::SCATTER_DIRECT)
+        return fail(h, MPM_ERR_UNSUPPORTED, "mpm_set_kernel_config: config %d scatters into a dense grid", config);
     h->eng.set_config(config);
     return MPM_OK;
 }

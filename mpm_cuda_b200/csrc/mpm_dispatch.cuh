@@ -11,10 +11,12 @@ namespace mpm {
 using FusedFn = void (*)(ParticleBuf, FusedArgs);
 using SurFn = void (*)(ParticleBuf, FusedArgs, SurArgs);
 
-// k_g2p2g<dim, mat, kFusedCfgs[ci], fixed_scene>; fixed_scene: one scene whose
-// parameters do not change during the run, passed in FusedArgs::scene
-FusedFn fused_fn(int dim, int mat, int ci, bool fixed_scene);
-// k_g2p2g_sur with `cta` threads (64 or 128), fixed_scene (3D jello)
-SurFn sur_fn(int cta, bool fixed_scene);
+// k_g2p2g<dim, mat, kFusedCfgs[ci], fixed_scene, paged>; fixed_scene: one
+// scene whose parameters do not change during the run, passed in
+// FusedArgs::scene; paged: a paged grid (direct-scatter configurations only:
+// nullptr for the others)
+FusedFn fused_fn(int dim, int mat, int ci, bool fixed_scene, bool paged);
+// k_g2p2g_sur with `cta` threads (64 or 128), fixed_scene, paged (3D jello)
+SurFn sur_fn(int cta, bool fixed_scene, bool paged);
 
 }  // namespace mpm

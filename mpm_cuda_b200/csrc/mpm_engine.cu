@@ -34,6 +34,7 @@ enum {
     CNT_FALLBACK = 8,
     CNT_REBINS = 9,
     CNT_UPDATE_DONE = 10,
+    CNT_POOL_FREE = 11,  // paged grid: height of the free stack
     CNT_N = 16
 };
 
@@ -82,6 +83,18 @@ __global__ void k_gather_positions(const float* __restrict__ s, const uint32_t* 
 }
 
 unsigned grid_blocks(long long n, int threads) { return (unsigned)std::max<long long>(1, (n + threads - 1) / threads); }
+
+// a[i] = value (the page table's "no page")
+__global__ void k_fill_int(int* __restrict__ a, long long n, int value) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = value;
+}
+
+// the free stack of a fresh pool: every physical block, the lowest on top
+__global__ void k_fill_stack(int* __restrict__ s, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) s[i] = (int)(n - 1 - i);
+}
 
 }  // namespace
 
@@ -133,6 +146,15 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     }
     if (opt.stress_mode != MPM_STRESS_PLAIN) {
         msg = "mpm_create: select the surrogate stress with mpm_set_stress_mode after creation";
+        return MPM_ERR_UNSUPPORTED;
+    }
+    if (opt.grid_pool_blocks < 0) {
+        msg = "mpm_create: grid_pool_blocks must be >= 0";
+        return MPM_ERR_INVALID;
+    }
+    paged = opt.grid_pool_blocks > 0;
+    if (paged && opt.p2g_mode != MPM_P2G_ATOMIC) {
+        msg = "mpm_create: a paged grid runs in MPM_P2G_ATOMIC only";
         return MPM_ERR_UNSUPPORTED;
     }
     char buf[512];
@@ -331,7 +353,14 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     // the device scene table never changes in such a run (only adaptive dt
     // writes it), so the fused kernels may carry the scene in their parameters
     fixed_scene = scenes_h.size() == 1 && !opt.adaptive_dt;
-    const size_t grid_bytes = (size_t)total_blocks * 64 * sizeof(float4);
+    if (paged) {
+        pool_cap = std::min<long long>(opt.grid_pool_blocks, total_blocks);
+        pages.trash = (int)pool_cap;
+        if ((rc = alloc((void**)&pages.page, total_blocks * sizeof(int), "page table")) != MPM_OK) return rc;
+        if ((rc = alloc((void**)&pages.slot_block, pool_cap * sizeof(int), "pool map")) != MPM_OK) return rc;
+        if ((rc = alloc((void**)&pages.free_slots, pool_cap * sizeof(int), "free blocks")) != MPM_OK) return rc;
+    }
+    const size_t grid_bytes = (size_t)grid_blocks_alloc() * 64 * sizeof(float4);
     if ((rc = alloc((void**)&grid_mom, grid_bytes, "grid_mom")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&grid_vel, grid_bytes, "grid_vel")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&err_d, sizeof(unsigned), "err")) != MPM_OK) return rc;
@@ -344,12 +373,16 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     for (int m = 0; m < kMats; ++m)
         if (mat_present[m]) mat_slots.s[m] = mat_slots.n++;
     mat_slots.n = std::max(mat_slots.n, 1);
-    const long long n_cell_counts = total_blocks * 64 * mat_slots.n;
+    // the binning's cell counters live at the physical block in a paged grid
+    const long long n_cell_counts = grid_blocks_alloc() * 64 * mat_slots.n;
     if ((rc = alloc((void**)&cell_count, n_cell_counts * sizeof(int), "cell counts")) != MPM_OK) return rc;
-    if ((rc = alloc((void**)&cell_end, total_blocks * 64 * sizeof(int), "cell ends")) != MPM_OK) return rc;
+    // the deterministic path's buffers (it needs a dense grid)
+    if ((rc = alloc((void**)&cell_end, paged ? 16 : total_blocks * 64 * sizeof(int), "cell ends")) != MPM_OK)
+        return rc;
     {
         const int src_planes = dim == 3 ? SrcPlanes<3>::COUNT : SrcPlanes<2>::COUNT;
-        if ((rc = alloc((void**)&det_src, (size_t)src_planes * cap * sizeof(float), "source records")) != MPM_OK)
+        if ((rc = alloc((void**)&det_src, paged ? 16 : (size_t)src_planes * cap * sizeof(float), "source records")) !=
+            MPM_OK)
             return rc;
     }
     if ((rc = alloc((void**)&seg_count, total_blocks * 4 * sizeof(int), "segment counts")) != MPM_OK) return rc;
@@ -389,10 +422,21 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     if (e == cudaSuccess) e = cudaMemset(err_d, 0, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(blk_flag, 0, total_blocks * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(cell_count, 0, n_cell_counts * sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(cell_end, 0, total_blocks * 64 * sizeof(int));
+    if (e == cudaSuccess && !paged) e = cudaMemset(cell_end, 0, total_blocks * 64 * sizeof(int));
+    if (e == cudaSuccess && paged) {
+        k_fill_int<<<grid_blocks(total_blocks, 256), 256>>>(pages.page, total_blocks, pages.trash);
+        k_fill_stack<<<grid_blocks(pool_cap, 256), 256>>>(pages.free_slots, pool_cap);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemset(pages.slot_block, 0xff, pool_cap * sizeof(int));
+    }
     if (e == cudaSuccess) e = cudaMemset(seg_count, 0, total_blocks * 4 * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(blk_epoch, 0xff, total_blocks * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(counters, 0, CNT_N * sizeof(int));
+    if (e == cudaSuccess && paged) {
+        const int free0 = (int)pool_cap;
+        e = cudaMemcpy(counters + CNT_POOL_FREE, &free0, sizeof(int), cudaMemcpyHostToDevice);
+        pages.n_free = counters + CNT_POOL_FREE;
+    }
     if (e == cudaSuccess) e = cudaMemset(speed_max, 0, scenes_h.size() * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(scene_time, 0, scenes_h.size() * sizeof(double));
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -402,6 +446,10 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     }
     update_ctas = (int)std::max<long long>(1, std::min<long long>((total_blocks + 3) / 4, (long long)num_sms * 8));
     cfg = (opt.kernel_config >= 0 && opt.kernel_config < kNumFusedCfgs) ? opt.kernel_config : 1;
+    if (paged && kFusedCfgs[cfg].scatter != SCATTER_DIRECT) {
+        msg = "mpm_create: the segmented scatter addresses a dense grid; choose another kernel_config";
+        return MPM_ERR_UNSUPPORTED;
+    }
     set_config(cfg);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
@@ -432,7 +480,11 @@ void Engine::set_config(int ci) {
     const int dyn = fused_dyn_smem(dim, kFusedCfgs[ci].kernel);
     for (int mat = 0; mat < kMats; ++mat) {
         int per_sm = 0;
-        const FusedFn fn = fused_fn(dim, mat, ci, fixed_scene);
+        const FusedFn fn = fused_fn(dim, mat, ci, fixed_scene, paged);
+        if (!fn) {  // a configuration the paged grid has no kernel for (rejected before)
+            fused_ctas[mat] = num_sms;
+            continue;
+        }
         // the segmented scatter's staging buffer can exceed the 48 KB a kernel
         // gets without opting in; a failure here shows in the occupancy query
         if (dyn > 0 && cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) != cudaSuccess)
@@ -460,10 +512,11 @@ void Engine::sur_occupancy() {
         int per_sm = 0;
         // the network rows live in dynamic shared memory; with the windows and
         // weights they can exceed the 48 KB a kernel gets without opting in
-        if (cudaFuncSetAttribute(sur_fn(ch, fixed_scene), cudaFuncAttributeMaxDynamicSharedMemorySize, sur_dyn_smem(ch)) !=
+        if (cudaFuncSetAttribute(sur_fn(ch, fixed_scene, paged), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 sur_dyn_smem(ch)) !=
             cudaSuccess)
             cudaGetLastError();  // not fatal here: the occupancy query and the launch report it
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sur_fn(ch, fixed_scene), ch, sur_dyn_smem(ch)) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sur_fn(ch, fixed_scene, paged), ch, sur_dyn_smem(ch)) !=
             cudaSuccess) {
             cudaGetLastError();
             per_sm = 1;
@@ -478,12 +531,14 @@ namespace {
 struct TuneKey {
     int device, dim, mats;
     long long particles, blocks;
+    bool paged;  // a paged grid has its own kernels (and no segmented scatter)
     bool operator<(const TuneKey& o) const {
         if (device != o.device) return device < o.device;
         if (dim != o.dim) return dim < o.dim;
         if (mats != o.mats) return mats < o.mats;
         if (particles != o.particles) return particles < o.particles;
-        return blocks < o.blocks;
+        if (blocks != o.blocks) return blocks < o.blocks;
+        return paged < o.paged;
     }
 };
 std::map<TuneKey, int>& tune_cache() {
@@ -543,6 +598,7 @@ int Engine::autotune(int steps, float* best_ms) {
     std::vector<float> best_of(kNumFusedCfgs, 1e30f);
     for (int it = 0; it < 2 * kNumFusedCfgs && e == cudaSuccess && rc == MPM_OK; ++it) {
         const int ci = it % kNumFusedCfgs;
+        if (paged && kFusedCfgs[ci].scatter != SCATTER_DIRECT) continue;  // the paged grid scatters directly
         e = cudaMemcpyAsync(st[cur], bk_state, state_bytes, cudaMemcpyDeviceToDevice, stream);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(scenes_d, bk_scenes.data(), bk_scenes.size() * sizeof(SceneParams),
@@ -595,7 +651,7 @@ int Engine::autotune(int steps, float* best_ms) {
     int mats = 0;
     for (int m = 0; m < kMats; ++m) mats |= mat_present[m] ? (1 << m) : 0;
     std::lock_guard<std::mutex> lk(tune_mutex());
-    tune_cache()[TuneKey{device, dim, mats, n_particles, total_blocks}] = best;
+    tune_cache()[TuneKey{device, dim, mats, n_particles, total_blocks, paged}] = best;
     return MPM_OK;
 }
 
@@ -603,7 +659,7 @@ int Engine::cached_config() const {
     int mats = 0;
     for (int m = 0; m < kMats; ++m) mats |= mat_present[m] ? (1 << m) : 0;
     std::lock_guard<std::mutex> lk(tune_mutex());
-    auto it = tune_cache().find(TuneKey{device, dim, mats, n_particles, total_blocks});
+    auto it = tune_cache().find(TuneKey{device, dim, mats, n_particles, total_blocks, paged});
     return it == tune_cache().end() ? -1 : it->second;
 }
 
@@ -621,8 +677,10 @@ void Engine::release() {
     }
     void* ptrs[] = {groups_d, scenes_d, grid_mom, grid_vel, err_d, keys[0], keys[1], vals[0], vals[1],
                     cell_count, seg_count, seg_start, sort_tmp, blk_flag, active, blk_epoch, counters, chunks,
-                    scan_tmp, pos_out, cell_end, det_src, sur_counts, speed_max, scene_time};
+                    scan_tmp, pos_out, cell_end, det_src, sur_counts, speed_max, scene_time,
+                    pages.page, pages.slot_block, pages.free_slots};
     for (void* p : ptrs) cudaFree(p);
+    pages = GridPages{};
     groups_d = nullptr;
     scenes_d = nullptr;
     grid_mom = grid_vel = nullptr;
@@ -697,30 +755,33 @@ void Engine::enqueue_direct_substep() {
 // bins the particles of buffer `from` by (home block, material) into the
 // other buffer, in the configuration's order within each segment (counting
 // placement, no sort), and builds the chunk lists of the result
-void Engine::enqueue_rebin(int from) {
+void Engine::enqueue_rebin(int from, bool reclaim) {
     const int to = 1 - from;
     const long long n_segs = total_blocks * 4;
     int* rank = reinterpret_cast<int*>(vals[0]);
+    if (paged && reclaim) {
+        // blocks with nothing active near them give their physical block back
+        auto k = dim == 3 ? k_pool_reclaim<3> : k_pool_reclaim<2>;
+        k<<<grid_blocks(pool_cap, 256), 256, 0, stream>>>(pages, blk_flag, blk_epoch, counters + CNT_EPOCH, scenes_d,
+                                                          (int)scenes_h.size());
+        note_launch("k_pool_reclaim");
+    }
     cudaMemsetAsync(counters + CNT_CHUNKS, 0, kMats * sizeof(int), stream);
     const unsigned nb = grid_blocks(n_particles, 256);
     if (n_particles > 0) {
-        if (dim == 3)
-            k_bin_count<3><<<nb, 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d, mat_slots, keys[0], rank,
-                                                   cell_count, seg_count);
-        else
-            k_bin_count<2><<<nb, 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d, mat_slots, keys[0], rank,
-                                                   cell_count, seg_count);
+        auto k = dim == 3 ? (paged ? k_bin_count<3, true> : k_bin_count<3, false>)
+                          : (paged ? k_bin_count<2, true> : k_bin_count<2, false>);
+        k<<<nb, 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d, mat_slots, keys[0], rank, cell_count,
+                                  seg_count, pages);
         note_launch("k_bin_count");
     }
     cub::DeviceScan::ExclusiveSum(scan_tmp, scan_tmp_bytes, seg_count, seg_start, (int)n_segs, stream);
     note_launch("cub::DeviceScan::ExclusiveSum");
     if (n_particles > 0) {
-        if (dim == 3)
-            k_bin_place<3><<<nb, 256, 0, stream>>>(buf(from), buf(to), n_particles, keys[0], rank, cell_count,
-                                                   seg_count, seg_start, mat_slots, kFusedCfgs[cfg].order, err_d);
-        else
-            k_bin_place<2><<<nb, 256, 0, stream>>>(buf(from), buf(to), n_particles, keys[0], rank, cell_count,
-                                                   seg_count, seg_start, mat_slots, kFusedCfgs[cfg].order, err_d);
+        auto k = dim == 3 ? (paged ? k_bin_place<3, true> : k_bin_place<3, false>)
+                          : (paged ? k_bin_place<2, true> : k_bin_place<2, false>);
+        k<<<nb, 256, 0, stream>>>(buf(from), buf(to), n_particles, keys[0], rank, cell_count, seg_count, seg_start,
+                                  mat_slots, kFusedCfgs[cfg].order, err_d, pages);
         note_launch("k_bin_place");
     }
     if (dim == 3)
@@ -733,7 +794,8 @@ void Engine::enqueue_rebin(int from) {
                                                                        scenes_d, (int)scenes_h.size(), err_d);
     note_launch("k_make_chunks");
     if (n_particles > 0) {
-        k_bin_reset<<<nb, 256, 0, stream>>>(keys[0], n_particles, mat_slots, cell_count, seg_count);
+        auto k = paged ? k_bin_reset<true> : k_bin_reset<false>;
+        k<<<nb, 256, 0, stream>>>(keys[0], n_particles, mat_slots, cell_count, seg_count, pages);
         note_launch("k_bin_reset");
     }
     k_count_rebin<<<1, 1, 0, stream>>>(counters + CNT_REBINS);
@@ -769,6 +831,7 @@ FusedArgs Engine::fused_args(int mat, bool bump) {
     for (const GroupParams& g : groups_h)
         if (g.type == mat && ++n_of_mat == 1) A.group = g;
     A.one_group = n_of_mat == 1 ? 1 : 0;
+    A.pages = pages;
     return A;
 }
 
@@ -794,12 +857,15 @@ void Engine::enqueue_grid_update() {
     // cursors, so the fused launches append the next substep's blocks from zero
     cudaLaunchAttribute attr;
     const cudaLaunchConfig_t lc = pdl_config(update_ctas, 256, 0, stream, &attr);
-    auto k = dim == 3 ? (fixed_scene ? k_grid_update_active<3, true> : k_grid_update_active<3, false>)
-                      : (fixed_scene ? k_grid_update_active<2, true> : k_grid_update_active<2, false>);
+    auto k = paged ? (dim == 3 ? (fixed_scene ? k_grid_update_active<3, true, true> : k_grid_update_active<3, false, true>)
+                               : (fixed_scene ? k_grid_update_active<2, true, true> : k_grid_update_active<2, false, true>))
+                   : (dim == 3 ? (fixed_scene ? k_grid_update_active<3, true, false> : k_grid_update_active<3, false, false>)
+                               : (fixed_scene ? k_grid_update_active<2, true, false>
+                                              : k_grid_update_active<2, false, false>));
     const cudaError_t e = cudaLaunchKernelEx(&lc, k, grid_mom, grid_vel, (const int*)active, counters + CNT_ACTIVE,
                                              blk_flag, blk_epoch, (const int*)(counters + CNT_EPOCH),
                                              (const SceneParams*)scenes_d, n_scenes, counters + CNT_CURSOR, (int)kMats,
-                                             (unsigned*)(counters + CNT_UPDATE_DONE), scenes_h[0]);
+                                             (unsigned*)(counters + CNT_UPDATE_DONE), scenes_h[0], pages, err_d);
     note_launch_status("k_grid_update_active", e);
 }
 
@@ -816,13 +882,13 @@ void Engine::enqueue_g2p2g(int parity) {
             As.rounds = chunk_particles() / ch;
             cudaLaunchAttribute attr;
             const cudaLaunchConfig_t lc = pdl_config(sur_ctas[mat], ch, sur_dyn_smem(ch), stream, &attr);
-            const cudaError_t e = cudaLaunchKernelEx(&lc, sur_fn(ch, fixed_scene), buf(parity), As, SA);
+            const cudaError_t e = cudaLaunchKernelEx(&lc, sur_fn(ch, fixed_scene, paged), buf(parity), As, SA);
             note_launch_status("k_g2p2g_sur", e);
         } else {
             cudaLaunchAttribute attr;
             const cudaLaunchConfig_t lc = pdl_config(fused_ctas[mat], kFusedCfgs[cfg].chunk,
                                                      fused_dyn_smem(dim, kFusedCfgs[cfg].kernel), stream, &attr);
-            const cudaError_t e = cudaLaunchKernelEx(&lc, fused_fn(dim, mat, cfg, fixed_scene), buf(parity), A);
+            const cudaError_t e = cudaLaunchKernelEx(&lc, fused_fn(dim, mat, cfg, fixed_scene, paged), buf(parity), A);
             note_launch_status("k_g2p2g", e);
             note_launch("fused_fn");
         }
@@ -919,16 +985,23 @@ bool Engine::defer_vc_now() const { return true; }
 int Engine::recover_vc() {
     if (!vc_deferred) return MPM_OK;
     if (n_particles > 0) {
-        if (dim == 3)
-            k_recover_vc<3><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(cur), n_particles, groups_d,
-                                                                               scenes_d, grid_vel);
-        else
-            k_recover_vc<2><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(cur), n_particles, groups_d,
-                                                                               scenes_d, grid_vel);
+        auto k = dim == 3 ? (paged ? k_recover_vc<3, true> : k_recover_vc<3, false>)
+                          : (paged ? k_recover_vc<2, true> : k_recover_vc<2, false>);
+        k<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(cur), n_particles, groups_d, scenes_d, grid_vel,
+                                                             pages);
         MPM_CUDA_TRY(cudaGetLastError(), "v/C recovery launch");
     }
     vc_deferred = false;
     return MPM_OK;
+}
+
+// paged grid: a physical block for every block a particle's stencil covers
+void Engine::enqueue_page_in_particles() {
+    if (n_particles == 0) return;
+    auto k = dim == 3 ? k_page_in_particles<3> : k_page_in_particles<2>;
+    k<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(cur), n_particles, groups_d, scenes_d, grid_mom, grid_vel,
+                                                         pages, err_d);
+    note_launch("k_page_in_particles");
 }
 
 // makes grid_mom hold the P2G of the current state (binned path): sorts the
@@ -938,7 +1011,7 @@ int Engine::prologue() {
         const int rc = recover_vc();
         if (rc != MPM_OK) return rc;
     }
-    const size_t grid_bytes = (size_t)total_blocks * 64 * sizeof(float4);
+    const size_t grid_bytes = (size_t)grid_blocks_alloc() * 64 * sizeof(float4);
     MPM_CUDA_TRY(cudaMemsetAsync(grid_mom, 0, grid_bytes, stream), "prologue clear");
     MPM_CUDA_TRY(cudaMemsetAsync(blk_flag, 0, total_blocks * sizeof(unsigned), stream), "prologue flags");
     MPM_CUDA_TRY(cudaMemsetAsync(counters + CNT_ACTIVE, 0, sizeof(int), stream), "prologue counters");
@@ -951,16 +1024,15 @@ int Engine::prologue() {
         grid_dirty = false;
         return MPM_OK;
     }
-    enqueue_rebin(cur);
+    if (paged) enqueue_page_in_particles();  // the binning counts and the P2G below need the pages
+    enqueue_rebin(cur, false);
     cur = 1 - cur;
     steps_since_rebin = 0;
     if (n_particles > 0) {
-        if (dim == 3)
-            k_p2g_prologue<3><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(
-                buf(cur), n_particles, groups_d, scenes_d, grid_mom, blk_flag, active, counters + CNT_ACTIVE, err_d);
-        else
-            k_p2g_prologue<2><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(
-                buf(cur), n_particles, groups_d, scenes_d, grid_mom, blk_flag, active, counters + CNT_ACTIVE, err_d);
+        auto k = dim == 3 ? (paged ? k_p2g_prologue<3, true> : k_p2g_prologue<3, false>)
+                          : (paged ? k_p2g_prologue<2, true> : k_p2g_prologue<2, false>);
+        k<<<grid_blocks(n_particles, 128), 128, 0, stream>>>(buf(cur), n_particles, groups_d, scenes_d, grid_mom,
+                                                             blk_flag, active, counters + CNT_ACTIVE, err_d, pages);
     }
     note_launch("k_p2g_prologue");
     int lrc = take_launch_error();
@@ -1276,13 +1348,37 @@ int Engine::set_state(int scene, const float* x, const float* v, const float* C,
     return MPM_OK;
 }
 
+// the scene's grid velocities in the dense blocked order (a paged block
+// without a page reads as zero)
+int Engine::download_grid(const SceneParams& sc, std::vector<float4>& blk) {
+    blk.assign((size_t)sc.n_nodes, make_float4(0.f, 0.f, 0.f, 0.f));
+    if (!paged) {
+        MPM_CUDA_TRY(cudaMemcpy(blk.data(), grid_vel + sc.node_off, sc.n_nodes * sizeof(float4), cudaMemcpyDeviceToHost),
+                     "grid download");
+        return MPM_OK;
+    }
+    std::vector<int> page((size_t)sc.n_blocks);
+    std::vector<float4> pool((size_t)pool_cap * 64);
+    MPM_CUDA_TRY(cudaMemcpy(page.data(), pages.page + sc.block_off, sc.n_blocks * sizeof(int), cudaMemcpyDeviceToHost),
+                 "page table download");
+    MPM_CUDA_TRY(cudaMemcpy(pool.data(), grid_vel, pool.size() * sizeof(float4), cudaMemcpyDeviceToHost),
+                 "grid pool download");
+    for (long long b = 0; b < sc.n_blocks; ++b)
+        if (page[b] >= 0 && page[b] < pages.trash)
+            std::copy(pool.begin() + (size_t)page[b] * 64, pool.begin() + (size_t)page[b] * 64 + 64,
+                      blk.begin() + (size_t)b * 64);
+    return MPM_OK;
+}
+
 int Engine::get_grid(int scene, float* mass, float* vel) {
     MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
     MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
     const SceneParams& sc = scenes_h[scene];
-    std::vector<float4> blk((size_t)sc.n_nodes);
-    MPM_CUDA_TRY(cudaMemcpy(blk.data(), grid_vel + sc.node_off, sc.n_nodes * sizeof(float4), cudaMemcpyDeviceToHost),
-                 "grid download");
+    std::vector<float4> blk;
+    {
+        const int rc = download_grid(sc, blk);
+        if (rc != MPM_OK) return rc;
+    }
     if (!direct()) {
         // blocks not stamped by the last grid update hold stale values
         std::vector<int> ep((size_t)sc.n_blocks);
@@ -1325,6 +1421,20 @@ int Engine::count_active_nodes(int scene, int64_t* n) {
     return MPM_OK;
 }
 
+int Engine::grid_pool(int64_t* capacity, int64_t* in_use) {
+    MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    int n_free = 0;
+    if (paged) {
+        MPM_CUDA_TRY(cudaMemcpyAsync(&n_free, counters + CNT_POOL_FREE, sizeof(int), cudaMemcpyDeviceToHost, stream),
+                     "pool counter download");
+        MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
+    }
+    const long long cap_blocks = paged ? pool_cap : total_blocks;
+    if (capacity) *capacity = cap_blocks;
+    if (in_use) *in_use = cap_blocks - n_free;
+    return MPM_OK;
+}
+
 int Engine::bin_stats(int64_t* fallbacks, int64_t* rebins) {
     MPM_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
     MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
@@ -1336,6 +1446,10 @@ int Engine::bin_stats(int64_t* fallbacks, int64_t* rebins) {
 }
 
 int Engine::set_p2g_mode(int mode) {
+    if (paged && mode != MPM_P2G_ATOMIC) {
+        last_error = "mpm_set_p2g_mode: a paged grid runs in MPM_P2G_ATOMIC only";
+        return MPM_ERR_UNSUPPORTED;
+    }
     if (opt.adaptive_dt && mode != MPM_P2G_ATOMIC) {
         last_error = "mpm_set_p2g_mode: adaptive dt runs in MPM_P2G_ATOMIC only";
         return MPM_ERR_UNSUPPORTED;

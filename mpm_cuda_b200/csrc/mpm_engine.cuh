@@ -89,6 +89,13 @@ struct Engine {
     // particles per chunk of the current configuration (CTA size x rounds)
     int chunk_particles() const;
     bool fixed_scene = false;        // one scene, fixed dt: fused kernels take it as a parameter
+    // paged grid (mpm_options.grid_pool_blocks > 0): the grid arrays hold
+    // pool_cap physical blocks plus the trash block; `pages` points at the
+    // device page table, the physical-to-virtual map and the free stack
+    bool paged = false;
+    long long pool_cap = 0;
+    GridPages pages{};
+    long long grid_blocks_alloc() const { return paged ? pool_cap + 1 : total_blocks; }
     // the state's v planes hold the last G2P positions and C is stale: the
     // fused kernels deferred them (k_recover_vc rebuilds both)
     bool vc_deferred = false;
@@ -139,6 +146,7 @@ struct Engine {
     int get_positions_async(int scene, float* out, long long* ticket);
     int wait_positions(long long ticket);
     int bin_stats(int64_t* fallbacks, int64_t* rebins);
+    int grid_pool(int64_t* capacity, int64_t* in_use);
     void set_config(int ci);
     int autotune(int steps, float* best_ms);
     int cached_config() const;
@@ -150,7 +158,9 @@ struct Engine {
     int take_launch_error();
     ParticleBuf buf(int p) const { return ParticleBuf{st[p], cap, gp[p], ids[p]}; }
     void enqueue_direct_substep();
-    void enqueue_rebin(int from);
+    void enqueue_rebin(int from, bool reclaim = true);
+    void enqueue_page_in_particles();
+    int download_grid(const SceneParams& sc, std::vector<float4>& blk);
     void enqueue_fused_substep(int parity);
     void enqueue_grid_update();
     void enqueue_adapt_dt();

@@ -5,6 +5,6 @@
 
 namespace mpm {
 
-FusedFn fused_fn_fixed(int dim, int mat, int ci) { return fused_table<true>(dim, mat, ci); }
+FusedFn fused_fn_fixed(int dim, int mat, int ci) { return fused_table<true, false>(dim, mat, ci); }
 
 }  // namespace mpm

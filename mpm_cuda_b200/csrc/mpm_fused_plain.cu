@@ -5,10 +5,12 @@
 
 namespace mpm {
 
-FusedFn fused_fn_fixed(int dim, int mat, int ci);  // mpm_fused_fixed.cu
+FusedFn fused_fn_fixed(int dim, int mat, int ci);         // mpm_fused_fixed.cu
+FusedFn fused_fn_paged(int dim, int mat, int ci, bool fixed);  // mpm_fused_paged.cu
 
-FusedFn fused_fn(int dim, int mat, int ci, bool fixed_scene) {
-    return fixed_scene ? fused_fn_fixed(dim, mat, ci) : fused_table<false>(dim, mat, ci);
+FusedFn fused_fn(int dim, int mat, int ci, bool fixed_scene, bool paged) {
+    if (paged) return fused_fn_paged(dim, mat, ci, fixed_scene);
+    return fixed_scene ? fused_fn_fixed(dim, mat, ci) : fused_table<false, false>(dim, mat, ci);
 }
 
 }  // namespace mpm

@@ -57,6 +57,77 @@ struct StencilIndex {
     __device__ __forceinline__ int operator()(int ox, int oy, int oz) const { return x[ox] + y[oy] + z[oz]; }
 };
 
+// ---------------------------------------------------------- paged grid --
+//
+// With PAGED = false every virtual block is its own physical block (the dense
+// grid) and none of the page machinery is compiled in.
+
+// physical block of virtual block v (trash when a paged block has no page;
+// a page being claimed by a concurrent page-in reads as trash too, so every
+// address formed from it stays inside the pool)
+template <bool PAGED>
+__device__ __forceinline__ long long phys_block(const GridPages& gp, long long v) {
+    if constexpr (PAGED) return min(gp.page[v], gp.trash);
+    else return v;
+}
+
+// Gives virtual block v a physical block if it has none: claims the page,
+// pops a free block and clears its momentum and velocity.  Several threads
+// of one kernel may ask for the same block; one claims it, the others see
+// the claim and return.  Kernels launched later see the page.  An empty pool
+// leaves v without a page and sets ERR_POOL.
+__device__ __forceinline__ void page_in(const GridPages& gp, long long v, float4* grid_mom, float4* grid_vel,
+                                        unsigned* err) {
+    int* pv = gp.page + v;
+    if (*pv != gp.trash) return;  // has a page, or another thread is claiming it
+    if (atomicCAS(pv, gp.trash, gp.trash + 1) != gp.trash) return;
+    const int t = atomicSub(gp.n_free, 1) - 1;
+    if (t < 0) {
+        atomicAdd(gp.n_free, 1);
+        atomicExch(pv, gp.trash);
+        atomicOr(err, ERR_POOL);
+        return;
+    }
+    const int slot = gp.free_slots[t];
+    gp.slot_block[slot] = (int)v;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int k = 0; k < 64; ++k) {
+        grid_mom[(long long)slot * 64 + k] = z;
+        grid_vel[(long long)slot * 64 + k] = z;
+    }
+    atomicExch(pv, slot);
+}
+
+// virtual block of node (ix, iy, iz) of scene sc and the node's index in it
+template <int D>
+__device__ __forceinline__ long long virtual_block(const SceneParams& sc, int ix, int iy, int iz, int& in) {
+    constexpr int S = BlockShape<D>::SHIFT;
+    constexpr int M = BlockShape<D>::SIDE - 1;
+    constexpr int SIDE = BlockShape<D>::SIDE;
+    in = (ix & M) + SIDE * ((iy & M) + SIDE * (iz & M));
+    return sc.block_off + (long long)(ix >> S) + (long long)sc.nb[0] * ((iy >> S) + (long long)sc.nb[1] * (iz >> S));
+}
+
+// index of node (ix, iy, iz) in the grid arrays (a node of a paged block
+// without a page lands in the trash block)
+template <int D, bool PAGED>
+__device__ __forceinline__ long long grid_node(const SceneParams& sc, const GridPages& gp, int ix, int iy, int iz) {
+    int in;
+    const long long v = virtual_block<D>(sc, ix, iy, iz, in);
+    return phys_block<PAGED>(gp, v) * 64 + in;
+}
+
+// value of node (ix, iy, iz); zero for a paged block without a page
+template <int D, bool PAGED>
+__device__ __forceinline__ float4 grid_read(const float4* g, const SceneParams& sc, const GridPages& gp, int ix, int iy,
+                                            int iz) {
+    int in;
+    const long long v = virtual_block<D>(sc, ix, iy, iz, in);
+    const long long b = phys_block<PAGED>(gp, v);
+    if (PAGED && b >= gp.trash) return make_float4(0.f, 0.f, 0.f, 0.f);
+    return g[b * 64 + in];
+}
+
 // scene owning global block `b` (binary search over block_off)
 __device__ __forceinline__ int scene_of_block(const SceneParams* scenes, int n_scenes, long long b) {
     int lo = 0, hi = n_scenes - 1;

@@ -86,11 +86,13 @@ __device__ __forceinline__ void home_of(const SceneParams& sc, const float* x, l
 
 // Pass 1: home block b, cell c and material m of every particle, its rank
 // among the particles of (b, m, c) and the size of segment (b, m).
-template <int D>
+// (PAGED: the cell counters of a block live at its physical block.)
+template <int D, bool PAGED>
 __global__ void __launch_bounds__(256) k_bin_count(ParticleBuf pb, long long n, const GroupParams* __restrict__ groups,
                                                    const SceneParams* __restrict__ scenes, MatSlots ms,
                                                    unsigned long long* __restrict__ key, int* __restrict__ rank,
-                                                   int* __restrict__ cell_count, int* __restrict__ seg_count) {
+                                                   int* __restrict__ cell_count, int* __restrict__ seg_count,
+                                                   GridPages gp) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float x[D];
@@ -101,7 +103,7 @@ __global__ void __launch_bounds__(256) k_bin_count(ParticleBuf pb, long long n, 
     long long b;
     int c;
     home_of<D>(sc, x, b, c);
-    rank[i] = atomicAdd(&cell_count[(b * ms.n + ms.s[g.type]) * 64 + c], 1);
+    rank[i] = atomicAdd(&cell_count[(phys_block<PAGED>(gp, b) * ms.n + ms.s[g.type]) * 64 + c], 1);
     atomicAdd(&seg_count[b * 4 + g.type], 1);
     key[i] = ((unsigned long long)b << 8) | ((unsigned long long)g.type << 6) | (unsigned long long)c;
 }
@@ -113,20 +115,20 @@ __global__ void __launch_bounds__(256) k_bin_count(ParticleBuf pb, long long n, 
 // and, cell-major, sum over c' < c of n_c' + r; the particle's state moves
 // there.  Ranks are exact, so the slots are a permutation of the segment; a
 // slot outside it (inconsistent counts) is reported, not written.
-template <int D>
+template <int D, bool PAGED>
 __global__ void __launch_bounds__(256) k_bin_place(ParticleBuf src, ParticleBuf dst, long long n,
                                                    const unsigned long long* __restrict__ key,
                                                    const int* __restrict__ rank, const int* __restrict__ cell_count,
                                                    const int* __restrict__ seg_count,
                                                    const int* __restrict__ seg_start, MatSlots ms, int cell_major,
-                                                   unsigned* __restrict__ err) {
+                                                   unsigned* __restrict__ err, GridPages gp) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const unsigned long long k = key[i];
     const long long b = (long long)(k >> 8);
     const int m = (int)((k >> 6) & 3), c = (int)(k & 63);
     const int r = rank[i];
-    const int4* cnt = reinterpret_cast<const int4*>(cell_count + (b * ms.n + ms.s[m]) * 64);
+    const int4* cnt = reinterpret_cast<const int4*>(cell_count + (phys_block<PAGED>(gp, b) * ms.n + ms.s[m]) * 64);
     int lower = 0, before = 0, cells_below = 0;
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
@@ -196,15 +198,16 @@ __global__ void __launch_bounds__(256) k_make_chunks(const int* __restrict__ seg
 }
 
 // zero the cell and segment counters that k_bin_count touched
-static __global__ void __launch_bounds__(256) k_bin_reset(const unsigned long long* __restrict__ key, long long n,
-                                                          MatSlots ms, int* __restrict__ cell_count,
-                                                          int* __restrict__ seg_count) {
+template <bool PAGED>
+__global__ void __launch_bounds__(256) k_bin_reset(const unsigned long long* __restrict__ key, long long n,
+                                                   MatSlots ms, int* __restrict__ cell_count,
+                                                   int* __restrict__ seg_count, GridPages gp) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const unsigned long long k = key[i];
     const long long b = (long long)(k >> 8);
     const int m = (int)((k >> 6) & 3);
-    cell_count[(b * ms.n + ms.s[m]) * 64 + (int)(k & 63)] = 0;
+    cell_count[(phys_block<PAGED>(gp, b) * ms.n + ms.s[m]) * 64 + (int)(k & 63)] = 0;
     seg_count[b * 4 + m] = 0;
 }
 
@@ -223,15 +226,42 @@ __device__ __forceinline__ long long block_of_node(const SceneParams& sc, int ix
     return sc.block_off + (long long)(ix >> S) + (long long)sc.nb[0] * ((iy >> S) + (long long)sc.nb[1] * (iz >> S));
 }
 
-// P2G of one particle straight to global memory, marking touched blocks
+// true when every block the stencil at `base` covers has a physical block
+// (the stencil spans at most 2 blocks per axis: its corner nodes decide)
 template <int D>
+__device__ __forceinline__ bool stencil_paged(const SceneParams& sc, const GridPages& gp, const int* base) {
+    bool ok = true;
+#pragma unroll
+    for (int c = 0; c < (D == 3 ? 8 : 4); ++c) {
+        int in;
+        const long long v = virtual_block<D>(sc, base[0] + 2 * (c & 1), base[1] + 2 * ((c >> 1) & 1),
+                                             D == 3 ? base[2] + 2 * (c >> 2) : 0, in);
+        ok = ok && phys_block<true>(gp, v) < gp.trash;
+    }
+    return ok;
+}
+
+// P2G of one particle straight to global memory, marking touched blocks.
+// PAGED: node addresses through the page table; a stencil reaching a block
+// without a page (the pool ran out, or a particle moved more than a cell in a
+// substep) sets ERR_POOL, and its writes land in the trash block.
+template <int D, bool PAGED = false>
 __device__ __forceinline__ void p2g_global(const Stencil<D>& st, const P2GSource<D>& src, const SceneParams& sc,
-                                           float4* grid_mom, unsigned* blk_flag, int* active, int* n_active) {
-    const StencilIndex<D> ix(sc, st.base);
-    float4* g = grid_mom + sc.node_off;
-    p2g_scatter<D>(st, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 c) {
-        atomicAdd(&g[ix(ox, oy, D == 3 ? oz : 0)], c);
-    });
+                                           float4* grid_mom, unsigned* blk_flag, int* active, int* n_active,
+                                           const GridPages& gp, unsigned* err_word) {
+    if constexpr (PAGED) {
+        if (!stencil_paged<D>(sc, gp, st.base)) atomicOr(err_word, ERR_POOL);
+        p2g_scatter<D>(st, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 c) {
+            atomicAdd(&grid_mom[grid_node<D, true>(sc, gp, st.base[0] + ox, st.base[1] + oy,
+                                                   D == 3 ? st.base[2] + oz : 0)], c);
+        });
+    } else {
+        const StencilIndex<D> ix(sc, st.base);
+        float4* g = grid_mom + sc.node_off;
+        p2g_scatter<D>(st, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 c) {
+            atomicAdd(&g[ix(ox, oy, D == 3 ? oz : 0)], c);
+        });
+    }
     // the stencil spans at most 2 blocks per axis: mark its corner blocks
 #pragma unroll
     for (int cx = 0; cx < 2; ++cx)
@@ -245,11 +275,11 @@ __device__ __forceinline__ void p2g_global(const Stencil<D>& st, const P2GSource
 }
 
 // First P2G of a state (after creation or set_state): direct atomics.
-template <int D>
+template <int D, bool PAGED>
 __global__ void __launch_bounds__(128) k_p2g_prologue(ParticleBuf pb, long long n, const GroupParams* __restrict__ groups,
                                                       const SceneParams* __restrict__ scenes, float4* __restrict__ grid_mom,
                                                       unsigned* __restrict__ blk_flag, int* __restrict__ active,
-                                                      int* __restrict__ n_active, unsigned* err_word) {
+                                                      int* __restrict__ n_active, unsigned* err_word, GridPages gp) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float x[D], v[D], C[D * D], F[D * D], aux;
@@ -264,7 +294,63 @@ __global__ void __launch_bounds__(128) k_p2g_prologue(ParticleBuf pb, long long 
     }
     P2GSource<D> src;
     particle_stress_source<D>(v, C, F, aux, g, sc, src);
-    p2g_global<D>(st, src, sc, grid_mom, blk_flag, active, n_active);
+    p2g_global<D, PAGED>(st, src, sc, grid_mom, blk_flag, active, n_active, gp, err_word);
+}
+
+// Paged grid: gives every block a particle's stencil covers a physical block
+// (before the first P2G of a state)
+template <int D>
+__global__ void __launch_bounds__(256) k_page_in_particles(ParticleBuf pb, long long n,
+                                                           const GroupParams* __restrict__ groups,
+                                                           const SceneParams* __restrict__ scenes,
+                                                           float4* __restrict__ grid_mom, float4* __restrict__ grid_vel,
+                                                           GridPages gp, unsigned* err_word) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float x[D];
+#pragma unroll
+    for (int a = 0; a < D; ++a) x[a] = pb.s[(Planes<D>::X + a) * pb.cap + i];
+    const SceneParams& sc = scenes[groups[pb.grp[i]].scene];
+    unsigned err = 0;
+    Stencil<D> st;
+    if (!make_stencil<D>(x, sc, st, err)) return;  // the P2G reports it
+#pragma unroll
+    for (int c = 0; c < (D == 3 ? 8 : 4); ++c) {
+        int in;
+        const long long v = virtual_block<D>(sc, st.base[0] + 2 * (c & 1), st.base[1] + 2 * ((c >> 1) & 1),
+                                             D == 3 ? st.base[2] + 2 * (c >> 2) : 0, in);
+        page_in(gp, v, grid_mom, grid_vel, err_word);
+    }
+}
+
+// Paged grid, at each re-binning: returns to the free stack the physical
+// block of every virtual block with nothing active in its 3^D neighbourhood
+// (no block there touched by the pending P2G nor stamped by the last two
+// grid updates).  Blocks next to active ones keep their pages: the next P2G
+// may reach them.  One thread per physical block.
+template <int D>
+__global__ void __launch_bounds__(256) k_pool_reclaim(GridPages gp, const unsigned* __restrict__ blk_flag,
+                                                      const int* __restrict__ blk_epoch, const int* __restrict__ epoch,
+                                                      const SceneParams* __restrict__ scenes, int n_scenes) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= gp.trash) return;
+    const int v = gp.slot_block[slot];
+    if (v < 0) return;
+    const int recent = *epoch - 2;
+    const SceneParams& sc = scenes[scene_of_block(scenes, n_scenes, v)];
+    const int lb = v - (int)sc.block_off;
+    const int b[3] = {lb % sc.nb[0], (lb / sc.nb[0]) % sc.nb[1], D == 3 ? lb / (sc.nb[0] * sc.nb[1]) : 0};
+    bool live = false;
+    for (int t = 0; t < (D == 3 ? 27 : 9) && !live; ++t) {
+        const int q[3] = {b[0] + t % 3 - 1, b[1] + (t / 3) % 3 - 1, D == 3 ? b[2] + t / 9 - 1 : 0};
+        if (q[0] < 0 || q[1] < 0 || q[2] < 0 || q[0] >= sc.nb[0] || q[1] >= sc.nb[1] || q[2] >= sc.nb[2]) continue;
+        const long long w = sc.block_off + q[0] + (long long)sc.nb[0] * (q[1] + (long long)sc.nb[1] * q[2]);
+        live = blk_flag[w] != 0u || blk_epoch[w] >= recent;
+    }
+    if (live) return;
+    gp.page[v] = gp.trash;
+    gp.slot_block[slot] = -1;
+    gp.free_slots[atomicAdd(gp.n_free, 1)] = slot;
 }
 
 // -------------------------------------------------------- grid update --
@@ -284,15 +370,18 @@ __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.lau
 // active-block count and the fused kernels' chunk cursors for the next pass
 // (every CTA has read the count before it counts itself done).
 // FIXED: the one scene of a fixed-dt run comes from the kernel parameters
-// (fixed_scene), as in the fused kernel.
-template <int D, bool FIXED>
+// (fixed_scene), as in the fused kernel.  PAGED: a block's nodes through its
+// physical block, and every neighbour of an updated block gets a physical
+// block (the next P2G reaches at most one block further).
+template <int D, bool FIXED, bool PAGED>
 __global__ void __launch_bounds__(256) k_grid_update_active(float4* __restrict__ grid_mom, float4* __restrict__ grid_vel,
                                                             const int* __restrict__ active, int* __restrict__ n_active,
                                                             unsigned* __restrict__ blk_flag, int* __restrict__ blk_epoch,
                                                             const int* __restrict__ epoch,
                                                             const SceneParams* __restrict__ scenes, int n_scenes,
                                                             int* __restrict__ cursors, int n_cursors,
-                                                            unsigned* __restrict__ done, SceneParams fixed_scene) {
+                                                            unsigned* __restrict__ done, SceneParams fixed_scene,
+                                                            GridPages gp, unsigned* __restrict__ err_word) {
     pdl_wait();
     const int na = *n_active;
     const int ep = *epoch;
@@ -302,10 +391,27 @@ __global__ void __launch_bounds__(256) k_grid_update_active(float4* __restrict__
         const SceneParams& sc = FIXED ? fixed_scene : scenes[scene_of_block(scenes, n_scenes, b)];
         int ix, iy, iz;
         block_node_coords<D>(sc, b - sc.block_off, lane, ix, iy, iz);
-        const long long gi = (long long)b * 64 + lane;
-        const float4 g = grid_mom[gi];
-        grid_vel[gi] = grid_node_update<D>(g, sc, ix, iy, iz);
-        grid_mom[gi] = make_float4(0.f, 0.f, 0.f, 0.f);
+        // (a block without a page -- the pool ran out -- may be claimed by a
+        // neighbour's page-in below while it is read here: any value from
+        // trash up means no page)
+        const long long pb = phys_block<PAGED>(gp, b);
+        if (!PAGED || pb < gp.trash) {
+            const long long gi = pb * 64 + lane;
+            const float4 g = grid_mom[gi];
+            grid_vel[gi] = grid_node_update<D>(g, sc, ix, iy, iz);
+            grid_mom[gi] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if constexpr (PAGED) {
+            if (lane < (D == 3 ? 27 : 9)) {
+                // neighbour (lane % 3 - 1, lane / 3 % 3 - 1, lane / 9 - 1) of this block
+                const int lb = b - (int)sc.block_off;
+                const int bx = lb % sc.nb[0] + lane % 3 - 1, by = (lb / sc.nb[0]) % sc.nb[1] + (lane / 3) % 3 - 1;
+                const int bz = D == 3 ? lb / (sc.nb[0] * sc.nb[1]) + lane / 9 - 1 : 0;
+                if (bx >= 0 && by >= 0 && bz >= 0 && bx < sc.nb[0] && by < sc.nb[1] && bz < sc.nb[2])
+                    page_in(gp, sc.block_off + bx + (long long)sc.nb[0] * (by + (long long)sc.nb[1] * bz), grid_mom,
+                            grid_vel, err_word);
+            }
+        }
         if (lane == 0) {
             blk_flag[b] = 0u;
             blk_epoch[b] = ep;
@@ -350,6 +456,7 @@ struct FusedArgs {
     // of loading each particle's group index and group record
     int one_group;
     GroupParams group;
+    GridPages pages;  // paged grid (the PAGED kernels)
 };
 
 // the group record of particle i of a fused launch
@@ -389,9 +496,11 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // starts the asynchronous copy of chunk c's grid-velocity window into tv
-// (zero outside the grid), NT threads
-template <int D, int NT>
-__device__ __forceinline__ void prefetch_velocity_tile(const FusedArgs& A, int c, float4* tv) {
+// (zero outside the grid), NT threads.  PAGED: through the page table (zero
+// for a block without a page), and the physical blocks of the window's 3^D
+// blocks (trash outside the scene) into s27 for the chunk's scatter.
+template <int D, int NT, bool PAGED>
+__device__ __forceinline__ void prefetch_velocity_tile(const FusedArgs& A, int c, float4* tv, int* s27) {
     constexpr int T = TileShape<D>::T;
     constexpr int S = BlockShape<D>::SHIFT;
     constexpr int M = BlockShape<D>::SIDE - 1;
@@ -399,6 +508,17 @@ __device__ __forceinline__ void prefetch_velocity_tile(const FusedArgs& A, int c
     const Chunk ch = A.chunks[c];
     const SceneParams& sc = A.scenes[ch.scene];
     const float4* g = A.grid_vel + sc.node_off;
+    if constexpr (PAGED) {
+        if ((int)threadIdx.x < (D == 3 ? 27 : 9)) {
+            const int t = threadIdx.x;
+            const int bx = (ch.o[0] + 1) / SIDE - 1 + t % 3, by = (ch.o[1] + 1) / SIDE - 1 + (t / 3) % 3;
+            const int bz = D == 3 ? (ch.o[2] + 1) / SIDE - 1 + t / 9 : 0;
+            const bool inb = bx >= 0 && by >= 0 && bz >= 0 && bx < sc.nb[0] && by < sc.nb[1] && bz < sc.nb[2];
+            s27[t] = inb ? (int)phys_block<true>(A.pages,
+                                                 sc.block_off + bx + (long long)sc.nb[0] * (by + (long long)sc.nb[1] * bz))
+                         : A.pages.trash;
+        }
+    }
     for (int t = threadIdx.x; t < TileShape<D>::N; t += NT) {
         const int tx = t % T, ty = (t / T) % T, tz = (D == 3) ? t / (T * T) : 0;
         const int ix = ch.o[0] + tx, iy = ch.o[1] + ty, iz = ch.o[2] + tz;
@@ -406,12 +526,19 @@ __device__ __forceinline__ void prefetch_velocity_tile(const FusedArgs& A, int c
         if (D == 3) in = in && iz >= 0 && iz < sc.n[2];
         const float4* src = A.grid_vel;  // not read when outside the grid
         if (in) {
-            // blocked node index relative to the scene (< 2^31 nodes), as in node_index
-            int idx = (ix >> S) * 64 + (ix & M) + ((iy >> S) * sc.nb[0] * 64 + (iy & M) * SIDE);
-            if (D == 3) idx += (iz >> S) * sc.nb[0] * sc.nb[1] * 64 + (iz & M) * SIDE * SIDE;
-            src = g + idx;
+            if constexpr (PAGED) {
+                int nin;
+                const long long pb = phys_block<true>(A.pages, virtual_block<D>(sc, ix, iy, iz, nin));
+                in = pb < A.pages.trash;
+                src = A.grid_vel + pb * 64 + nin;
+            } else {
+                // blocked node index relative to the scene (< 2^31 nodes), as in node_index
+                int idx = (ix >> S) * 64 + (ix & M) + ((iy >> S) * sc.nb[0] * 64 + (iy & M) * SIDE);
+                if (D == 3) idx += (iz >> S) * sc.nb[0] * sc.nb[1] * 64 + (iz & M) * SIDE * SIDE;
+                src = g + idx;
+            }
         }
-        cp_async16(&tv[tv_idx<D>(tx, ty, tz)], src, in);
+        cp_async16(&tv[tv_idx<D>(tx, ty, tz)], in ? src : A.grid_vel, in);
     }
 }
 
@@ -426,13 +553,19 @@ __device__ __forceinline__ bool in_window(const int* base, const int* o) {
 
 // G2P of one particle from the window, or from global memory for a particle
 // that drifted out of it since the last re-binning
-template <int D>
+template <int D, bool PAGED = false>
 __device__ __forceinline__ void g2p_window(const Stencil<D>& st, const int* o, const float4* tv, const SceneParams& sc,
                                            const FusedArgs& A, G2PAcc<D>& acc) {
     if (in_window<D>(st.base, o)) {
         const int b0 = st.base[0] - o[0], b1 = st.base[1] - o[1], b2 = D == 3 ? st.base[2] - o[2] : 0;
         g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) {
             return tv[tv_idx<D>(b0 + ox, b1 + oy, b2 + oz)];
+        }, acc);
+    } else if constexpr (PAGED) {
+        atomicAdd(A.fallback, 1u);
+        g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) {
+            return grid_read<D, true>(A.grid_vel, sc, A.pages, st.base[0] + ox, st.base[1] + oy,
+                                      D == 3 ? st.base[2] + oz : 0);
         }, acc);
     } else {
         atomicAdd(A.fallback, 1u);
@@ -513,19 +646,68 @@ __device__ __forceinline__ unsigned touched_bits(int l0, int l1, int l2) {
 // P2G scatter of the next substep straight to global memory with float4
 // reductions; a stencil inside the window records the blocks it covers in
 // `touched`, one outside it marks them itself
+// Node offsets of a stencil inside a chunk's window in a paged grid: for
+// node (ox, oy, oz), x[ox] + y[oy] + z[oz] packs the window block (0..26,
+// low byte) and the node inside it (bits 8..) of the physical address
+// s27[block] * 64 + node.
 template <int D>
+struct PagedStencilIndex {
+    int x[3], y[3], z[3];
+    __device__ __forceinline__ PagedStencilIndex(const int* base, const int* o) {
+        constexpr int S = BlockShape<D>::SHIFT;
+        constexpr int M = BlockShape<D>::SIDE - 1;
+        constexpr int SIDE = BlockShape<D>::SIDE;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            // window origin o = home block * SIDE - 1: block of node g relative
+            // to the one below the home block is (g >> S) - (o + 1) / SIDE + 1
+            const int gx = base[0] + k, gy = base[1] + k;
+            x[k] = ((gx >> S) - (o[0] + 1) / SIDE + 1) + ((gx & M) << 8);
+            y[k] = 3 * ((gy >> S) - (o[1] + 1) / SIDE + 1) + (((gy & M) * SIDE) << 8);
+            if (D == 3) {
+                const int gz = base[2] + k;
+                z[k] = 9 * ((gz >> S) - (o[2] + 1) / SIDE + 1) + (((gz & M) * SIDE * SIDE) << 8);
+            } else {
+                z[k] = 0;
+            }
+        }
+    }
+    // physical node index of stencil node (ox, oy, oz)
+    __device__ __forceinline__ long long operator()(const int* s27, int ox, int oy, int oz) const {
+        const int p = x[ox] + y[oy] + z[oz];
+        return (long long)s27[p & 255] * 64 + (p >> 8);
+    }
+};
+
+template <int D, bool PAGED = false>
 __device__ __forceinline__ void scatter_global(const Stencil<D>& sn, const P2GSource<D>& src, const SceneParams& sc,
-                                               const int* o, const FusedArgs& A, unsigned* touched) {
+                                               const int* o, const FusedArgs& A, unsigned* touched,
+                                               const int* s27 = nullptr) {
     if (in_window<D>(sn.base, o)) {
-        const StencilIndex<D> ix(sc, sn.base);
-        float4* g = A.grid_mom + sc.node_off;
-        p2g_scatter<D>(sn, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 cc) {
-            atomicAdd(&g[ix(ox, oy, D == 3 ? oz : 0)], cc);
-        });
+        if constexpr (PAGED) {
+            const PagedStencilIndex<D> ix(sn.base, o);
+            // a block the stencil covers has no page: the pool ran out or the
+            // particle moved more than a cell since the last grid update
+            bool ok = true;
+#pragma unroll
+            for (int c = 0; c < (D == 3 ? 8 : 4); ++c)
+                ok = ok && s27[(ix.x[2 * (c & 1)] + ix.y[2 * ((c >> 1) & 1)] + ix.z[D == 3 ? 2 * (c >> 2) : 0]) & 255] <
+                               A.pages.trash;
+            if (!ok) atomicOr(A.err_word, ERR_POOL);
+            p2g_scatter<D>(sn, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 cc) {
+                atomicAdd(&A.grid_mom[ix(s27, ox, oy, D == 3 ? oz : 0)], cc);
+            });
+        } else {
+            const StencilIndex<D> ix(sc, sn.base);
+            float4* g = A.grid_mom + sc.node_off;
+            p2g_scatter<D>(sn, src, sc.h, sc.inv_h, [&](int ox, int oy, int oz, float4 cc) {
+                atomicAdd(&g[ix(ox, oy, D == 3 ? oz : 0)], cc);
+            });
+        }
         atomicOr(touched, touched_bits<D>(sn.base[0] - o[0], sn.base[1] - o[1], D == 3 ? sn.base[2] - o[2] : 0));
     } else {
         atomicAdd(A.fallback, 1u);
-        p2g_global<D>(sn, src, sc, A.grid_mom, A.blk_flag, A.active, A.n_active);
+        p2g_global<D, PAGED>(sn, src, sc, A.grid_mom, A.blk_flag, A.active, A.n_active, A.pages, A.err_word);
     }
 }
 
@@ -576,7 +758,7 @@ __device__ __forceinline__ void scatter_segmented(bool valid, const Stencil<D>& 
     const bool inw = valid && in_window<D>(sn.base, o);
     if (valid && !inw) {
         atomicAdd(A.fallback, 1u);
-        p2g_global<D>(sn, src, sc, A.grid_mom, A.blk_flag, A.active, A.n_active);
+        p2g_global<D>(sn, src, sc, A.grid_mom, A.blk_flag, A.active, A.n_active, A.pages, A.err_word);
     }
     const unsigned part = __ballot_sync(FULL, inw);
     if (part == 0u) return;
@@ -669,9 +851,10 @@ struct SpeedFlush {
 // body's barrier.  Two barriers per chunk: (1) window landed, the chunk after
 // next and the cleared touched word published; (2) body done (touched
 // complete, window free).  Shared words of parity b = k & 1 are rewritten two
-// chunks later, after both barriers of the chunk in between.
-template <int D, int NT, bool FIXED = false, class Body, class Post>
-__device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][TileShape<D>::VN],
+// chunks later, after both barriers of the chunk in between.  PAGED: the
+// window's physical blocks (s27) are fetched with the window.
+template <int D, int NT, bool FIXED = false, bool PAGED = false, class Body, class Post>
+__device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][TileShape<D>::VN], int (&s27)[2][27],
                                            unsigned (&touched)[2], int (&s_cn)[2], Body body, Post post) {
     const int nch = *A.n_chunks;
     if (threadIdx.x == 0) {
@@ -681,11 +864,11 @@ __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][T
     __syncthreads();
     int cur = s_cn[0], nxt = s_cn[1];
     __syncthreads();  // s_cn is rewritten below
-    if (cur < nch) prefetch_velocity_tile<D, NT>(A, cur, tv[0]);
+    if (cur < nch) prefetch_velocity_tile<D, NT, PAGED>(A, cur, tv[0], s27[0]);
     cp_async_commit();
     for (int k = 0; cur < nch; ++k) {
         const int b = k & 1;
-        if (nxt < nch) prefetch_velocity_tile<D, NT>(A, nxt, tv[b ^ 1]);
+        if (nxt < nch) prefetch_velocity_tile<D, NT, PAGED>(A, nxt, tv[b ^ 1], s27[b ^ 1]);
         cp_async_commit();
         if (threadIdx.x == 0) {
             s_cn[b] = atomicAdd(A.cursor, 1);  // the chunk after next
@@ -697,7 +880,7 @@ __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][T
         const int si = ch.scene;
         const SceneParams& sc = chunk_scene<FIXED>(A, si);
         const int o[3] = {ch.o[0], ch.o[1], ch.o[2]};
-        body(ch, sc, o, tv[b], &touched[b]);
+        body(ch, sc, o, tv[b], &touched[b], s27[b]);
         __syncthreads();     // (2)
         mark_touched<D>(touched[b], sc, o, A);
         post(si);
@@ -716,11 +899,13 @@ __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][T
 // (SCATTER_DIRECT) or per run of a warp's lanes sharing a stencil base
 // (SCATTER_SEGMENTED, staging buffer in dynamic shared memory).  FIXED: the
 // scene comes from A.scene (one scene, dt fixed for the run).
-template <int D, int MAT, int CHUNK, int MINB, bool FIXED, int SCATTER>
+template <int D, int MAT, int CHUNK, int MINB, bool FIXED, int SCATTER, bool PAGED>
 __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs A) {
     using P = Planes<D>;
     using TS = TileShape<D>;
+    static_assert(!(PAGED && SCATTER == SCATTER_SEGMENTED), "the segmented scatter addresses a dense grid");
     __shared__ __align__(16) float4 tv[2][TS::VN];  // grid velocity windows (double-buffered)
+    __shared__ int s27[2][27];                      // PAGED: the windows' physical blocks
     __shared__ unsigned touched[2];                 // 3^D neighbour-block bits
     __shared__ int s_cn[2];
     __shared__ unsigned s_speed;                    // adaptive dt: this chunk's max signal speed
@@ -732,8 +917,9 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
     if (A.bump_epoch && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.epoch, 1);
     if (threadIdx.x == 0) s_speed = 0u;
     SpeedFlush speed;
-    chunk_loop<D, CHUNK, FIXED>(A, tv, touched, s_cn,
-                                [&](const Chunk& ch, const SceneParams& sc, const int* o, const float4* w, unsigned* tb) {
+    chunk_loop<D, CHUNK, FIXED, PAGED>(A, tv, s27, touched, s_cn,
+                                       [&](const Chunk& ch, const SceneParams& sc, const int* o, const float4* w,
+                                           unsigned* tb, const int* wpages) {
         unsigned speed_bits = 0u;
 #pragma unroll 1
         for (int r = 0; r < A.rounds; ++r) {
@@ -756,7 +942,7 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
                 Stencil<D> st;
                 if (make_stencil<D>(x, sc, st, err)) {
                     G2PAcc<D> acc;
-                    g2p_window<D>(st, o, w, sc, A, acc);
+                    g2p_window<D, PAGED>(st, o, w, sc, A, acc);
                     // loaded after the gather, its register peak
                     const GroupParams g = particle_group<FIXED>(A, pb, i);
                     float F[D * D], Cn[D * D], v[D], aux;
@@ -770,7 +956,7 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
                         if (MAT == SNOW) snow_stress_source<D>(v, Cn, esvd, aux, g, sc.dt_next, src);
                         else particle_stress_source<D, MAT>(v, Cn, F, aux, g, sc.dt_next, src);
                         if constexpr (SCATTER == SCATTER_SEGMENTED) scatter = true;
-                        else scatter_global<D>(sn, src, sc, o, A, tb);
+                        else scatter_global<D, PAGED>(sn, src, sc, o, A, tb, wpages);
                     }
                 }
                 if (err) atomicOr(A.err_word, err);
@@ -787,10 +973,10 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
 // the velocities it gathered (the next grid update has not run), so the same
 // gather gives the same v and C = 4/h B.  A particle whose stencil left the
 // grid (the pass reported it) keeps its planes.
-template <int D>
+template <int D, bool PAGED>
 __global__ void __launch_bounds__(256) k_recover_vc(ParticleBuf pb, long long n, const GroupParams* __restrict__ groups,
                                                     const SceneParams* __restrict__ scenes,
-                                                    const float4* __restrict__ grid_vel) {
+                                                    const float4* __restrict__ grid_vel, GridPages gp) {
     using P = Planes<D>;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -803,10 +989,16 @@ __global__ void __launch_bounds__(256) k_recover_vc(ParticleBuf pb, long long n,
     Stencil<D> st;
     unsigned err = 0;
     if (!make_stencil<D>(x0, sc, st, err)) return;
-    const StencilIndex<D> ix(sc, st.base);
-    const float4* g = grid_vel + sc.node_off;
     G2PAcc<D> acc;
-    g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) { return g[ix(ox, oy, D == 3 ? oz : 0)]; }, acc);
+    if constexpr (PAGED) {
+        g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) {
+            return grid_read<D, true>(grid_vel, sc, gp, st.base[0] + ox, st.base[1] + oy, D == 3 ? st.base[2] + oz : 0);
+        }, acc);
+    } else {
+        const StencilIndex<D> ix(sc, st.base);
+        const float4* g = grid_vel + sc.node_off;
+        g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) { return g[ix(ox, oy, D == 3 ? oz : 0)]; }, acc);
+    }
     const float c4 = 4.f * sc.inv_h;
 #pragma unroll
     for (int a = 0; a < D; ++a) {

@@ -35,7 +35,7 @@ struct SurArgs {
     unsigned long long* counts;  // [0] stresses from the network, [1] SVD fallbacks
 };
 
-template <int CHUNK, int MINB, bool FIXED>
+template <int CHUNK, int MINB, bool FIXED, bool PAGED>
 __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, FusedArgs A, SurArgs SA) {
     constexpr int D = 3;
     constexpr int MAT = JELLO;
@@ -43,6 +43,7 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
     static_assert(CHUNK % 32 == 0, "whole warps");
     constexpr int XS = kSurRowStride, SS = kSurStashStride;
     __shared__ __align__(16) float4 tv[2][TS::VN];  // grid velocity windows (double-buffered)
+    __shared__ int s27[2][27];                      // PAGED: the windows' physical blocks
     __shared__ __align__(16) mlp::Forward W;        // network weights
     extern __shared__ float sxy[];                  // CHUNK network rows (inputs, then outputs), CHUNK stash rows
     __shared__ unsigned touched[2];
@@ -63,8 +64,9 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
     unsigned n_net = 0, n_svd = 0;
     if (threadIdx.x == 0) s_speed = 0u;
     SpeedFlush speed;
-    chunk_loop<D, CHUNK, FIXED>(A, tv, touched, s_cn,
-                                [&](const Chunk& ch, const SceneParams& sc, const int* o, const float4* w, unsigned* tb) {
+    chunk_loop<D, CHUNK, FIXED, PAGED>(A, tv, s27, touched, s_cn,
+                                       [&](const Chunk& ch, const SceneParams& sc, const int* o, const float4* w,
+                                           unsigned* tb, const int* wpages) {
         unsigned speed_bits = 0u;
         // every thread runs every round (the network step is warp-synchronous)
 #pragma unroll 1
@@ -85,7 +87,7 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
                 Stencil<D> st;
                 if (make_stencil<D>(x, sc, st, err)) {
                     G2PAcc<D> acc;
-                    g2p_window<D>(st, o, w, sc, A, acc);
+                    g2p_window<D, PAGED>(st, o, w, sc, A, acc);
                     const GroupParams g = A.groups[gi];
                     float F[D * D], Cn[D * D], v[D], aux;
                     err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux, nullptr,
@@ -150,7 +152,7 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
                     particle_stress_source<D, MAT>(v, Cn, F, 1.f, g, sc.dt_next, src);
                     ++n_svd;
                 }
-                scatter_global<D>(sn, src, sc, o, A, tb);
+                scatter_global<D, PAGED>(sn, src, sc, o, A, tb, wpages);
             }
             if (err) atomicOr(A.err_word, err);
             __syncwarp();  // the rows are rewritten by the next round

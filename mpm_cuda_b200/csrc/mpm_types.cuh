@@ -9,7 +9,8 @@ namespace mpm {
 // material type values match the reference enum (Elasiticity.cuh:10-11)
 enum : int { JELLO = 0, SNOW = 1, WATER = 2, SAND = 3 };
 enum : int { BC_STICKY = 0, BC_SLIP = 1, BC_SEPARATE = 2 };
-enum : unsigned { ERR_OUT_OF_GRID = 1u, ERR_NONFINITE = 2u, ERR_DET = 4u, ERR_BINNING = 8u, ERR_TIMEOUT = 16u };
+enum : unsigned { ERR_OUT_OF_GRID = 1u, ERR_NONFINITE = 2u, ERR_DET = 4u, ERR_BINNING = 8u, ERR_TIMEOUT = 16u,
+                  ERR_POOL = 32u };
 
 // One particle group: material + per-particle mass/volume (ParticleGroup,
 // MPMSimulator.cuh:30-52; Material, Elasiticity.cuh:19-45).
@@ -69,6 +70,20 @@ struct Planes {
     static constexpr int F = 2 * D + D * D;
     static constexpr int AUX = 2 * D + 2 * D * D;
     static constexpr int COUNT = 2 * D + 2 * D * D + 1;
+};
+
+// Paged grid (mpm_options.grid_pool_blocks > 0).  The grid arrays hold a
+// pool of `trash` physical 64-node blocks plus one trash block (index
+// `trash`); page[v] is the physical block of virtual block v (the dense
+// block index, scene block_off included) or `trash` when v has none.  Every
+// address a kernel forms stays inside the pool: a block without a page reads
+// as empty and writes land in the trash block, which nothing reads.
+struct GridPages {
+    int* page;        // [virtual blocks]
+    int* slot_block;  // [trash]: virtual block of each physical block, -1 when free
+    int* free_slots;  // stack of free physical blocks
+    int* n_free;      // its height
+    int trash;        // pool capacity = index of the trash block
 };
 
 struct ParticleBuf {

@@ -138,7 +138,7 @@ class Simulation:
     def __init__(self, scenes: Sequence[Scene], p2g_mode: int = L.P2G_ATOMIC,
                  stress_mode: int = L.STRESS_PLAIN, use_graph: bool = True, device: int = 0,
                  rebin_interval: int = 0, kernel_config: int = -1, adaptive_dt: bool = False,
-                 cfl: float = 0.5):
+                 cfl: float = 0.5, grid_pool_blocks: int = 0):
         lib = L.load()
         self.scenes = list(scenes)
         self.dim = self.scenes[0].dim
@@ -151,6 +151,7 @@ class Simulation:
         opt.kernel_config = kernel_config
         opt.adaptive_dt = int(adaptive_dt)
         opt.cfl = cfl
+        opt.grid_pool_blocks = grid_pool_blocks
         h = C.c_void_p()
         L.check(lib.mpm_create(sdescs, len(self.scenes), C.byref(opt), C.byref(h)))
         self._h = h
@@ -303,6 +304,12 @@ class Simulation:
         c, ms = C.c_int(), C.c_float()
         self._check(self._lib.mpm_autotune(self._h, n_substeps, C.byref(c), C.byref(ms)))
         return c.value, ms.value
+
+    def grid_pool(self):
+        """(pool capacity, blocks in use) of the grid, in 64-node blocks."""
+        cap, used = C.c_int64(), C.c_int64()
+        self._check(self._lib.mpm_get_grid_pool(self._h, C.byref(cap), C.byref(used)))
+        return cap.value, used.value
 
     def bin_stats(self):
         """(fallback gathers/scatters served from global memory, re-binnings)."""

@@ -38,7 +38,7 @@ def test_struct_sizes_match_header_layout():
     # natural alignment of the C structs in include/mpm_b200.h
     assert C.sizeof(L.MaterialDesc) == 8 + 8 * 8
     assert C.sizeof(L.GroupDesc) == 72 + 16 + 8 + 16 + 24 + 24
-    assert C.sizeof(L.Options) == 36
+    assert C.sizeof(L.Options) == 40
 
 
 def _mk(**kw):
@@ -58,6 +58,17 @@ def test_create_rejects_bad_scene(bad, code):
     with pytest.raises(L.MPMError) as e:
         Simulation([_mk(**bad)])
     assert e.value.code == code
+
+
+def test_paged_grid_options_are_checked_on_the_host():
+    # a negative pool, or a pool with a path that needs a dense grid: refused
+    # before any CUDA call
+    for kw, code in ((dict(grid_pool_blocks=-1), L.ERR_INVALID),
+                     (dict(grid_pool_blocks=64, p2g_mode=L.P2G_DIRECT), L.ERR_UNSUPPORTED),
+                     (dict(grid_pool_blocks=64, p2g_mode=L.P2G_DETERMINISTIC), L.ERR_UNSUPPORTED)):
+        with pytest.raises(L.MPMError) as e:
+            Simulation([S.c0_jello2d()], **kw)
+        assert e.value.code == code, kw
 
 
 def test_create_rejects_sand_and_bad_material():
