@@ -296,7 +296,8 @@ def run_ours(args, rank, world, local_rank, dist):
     n_part = sum(s.n_particles for s in scenes)
     from mpm_cuda_b200 import _lib as L
     mode = {"binned": L.P2G_ATOMIC, "direct": L.P2G_DIRECT}[args.mode]
-    sim = Simulation(scenes, device=local_rank, p2g_mode=mode, kernel_config=args.kernel_config)
+    sim = Simulation(scenes, device=local_rank, p2g_mode=mode, kernel_config=args.kernel_config,
+                     grid_pool_blocks=args.grid_pool_blocks)
     kcfg = sim.kernel_config()
     chunk, min_ctas, rounds = C.c_int(), C.c_int(), C.c_int()
     L.load().mpm_kernel_config_info(kcfg, C.byref(chunk), C.byref(min_ctas), C.byref(rounds))
@@ -319,6 +320,9 @@ def run_ours(args, rank, world, local_rank, dist):
 
     # per-kernel device time (separate launches, CUDA events on the same stream)
     fallbacks, rebins = sim.bin_stats()
+    pool_cap, pool_used = sim.grid_pool()
+    grid_desc = ("dense" if args.grid_pool_blocks == 0 else
+                 f"paged: {pool_used} of {pool_cap} pool blocks in use")
     stages = sim.profile_stages(20)
     active_nodes = sum(sim.count_active_nodes(i) for i in range(len(scenes)))
     sp = state_bytes_per_particle(scenes)
@@ -362,7 +366,8 @@ def run_ours(args, rank, world, local_rank, dist):
     d = scenes[0].dim
     host = [torch.empty((n_part, d), dtype=torch.float32, pin_memory=True).numpy() for _ in range(3)]
     e2e_scenes, _ = build_workload(args.workload, rank, world)
-    s3 = Simulation(e2e_scenes, device=local_rank, p2g_mode=mode, kernel_config=kcfg)
+    s3 = Simulation(e2e_scenes, device=local_rank, p2g_mode=mode, kernel_config=kcfg,
+                    grid_pool_blocks=args.grid_pool_blocks)
 
     def e2e_pass(n):
         """n substeps, each followed by its positions' copy to the host;
@@ -411,6 +416,7 @@ def run_ours(args, rank, world, local_rank, dist):
             "config": {"workload": desc, "particles_per_gpu": n_part, "particles_total": int(total_particles),
                        "active_nodes": active_nodes, "stress": "plain (SVD)", "path": args.mode,
                        "tile_fallbacks": fallbacks, "rebins": rebins,
+                       "grid": grid_desc,
                        "kernel_config": {"index": kcfg, "chunk": chunk.value, "min_ctas_per_sm": min_ctas.value,
                                          "particles_per_thread": rounds.value,
                                          "chosen_by": "autotuner" if args.kernel_config < 0 else "flag"},
@@ -517,6 +523,8 @@ def main():
     ap.add_argument("--kernel-config", type=int, default=-1, help="fused-kernel configuration; -1 = autotune")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-stress comparison")
+    ap.add_argument("--grid-pool-blocks", type=int, default=0,
+                    help="paged grid with a pool of this many 64-node blocks (0 = dense grid)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

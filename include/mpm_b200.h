@@ -168,7 +168,8 @@ typedef struct mpm_options {
                            is allocated densely (the reference allocates its
                            grid densely, MPMSimulator.cpp:122-146).  > 0: the
                            grid is paged: one pool of this many 64-node blocks
-                           shared by all scenes, pages
+                           (at most the scenes' block count) shared by all
+                           scenes, pages
                            assigned on the device to the blocks particles
                            touch and their neighbours and returned when nothing
                            is active near them; a step that needs more blocks
