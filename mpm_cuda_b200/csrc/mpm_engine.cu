@@ -755,7 +755,11 @@ void Engine::enqueue_direct_substep() {
 // bins the particles of buffer `from` by (home block, material) into the
 // other buffer, in the configuration's order within each segment (counting
 // placement, no sort), and builds the chunk lists of the result
-void Engine::enqueue_rebin(int from, bool reclaim) {
+void Engine::enqueue_rebin(int from, bool in_loop) {
+    // in_loop: a re-binning between two fused passes: the paged grid reclaims
+    // blocks, and the v and C planes, which the fused passes never read and the
+    // next one rewrites, stay behind
+    const bool reclaim = in_loop;
     const int to = 1 - from;
     const long long n_segs = total_blocks * 4;
     int* rank = reinterpret_cast<int*>(vals[0]);
@@ -781,7 +785,7 @@ void Engine::enqueue_rebin(int from, bool reclaim) {
         auto k = dim == 3 ? (paged ? k_bin_place<3, true> : k_bin_place<3, false>)
                           : (paged ? k_bin_place<2, true> : k_bin_place<2, false>);
         k<<<nb, 256, 0, stream>>>(buf(from), buf(to), n_particles, keys[0], rank, cell_count, seg_count, seg_start,
-                                  mat_slots, kFusedCfgs[cfg].order, err_d, pages);
+                                  mat_slots, kFusedCfgs[cfg].order, in_loop ? 0 : 1, err_d, pages);
         note_launch("k_bin_place");
     }
     if (dim == 3)

@@ -158,7 +158,7 @@ struct Engine {
     int take_launch_error();
     ParticleBuf buf(int p) const { return ParticleBuf{st[p], cap, gp[p], ids[p]}; }
     void enqueue_direct_substep();
-    void enqueue_rebin(int from, bool reclaim = true);
+    void enqueue_rebin(int from, bool in_loop = true);
     void enqueue_page_in_particles();
     int download_grid(const SceneParams& sc, std::vector<float4>& blk);
     void enqueue_fused_substep(int parity);

@@ -113,15 +113,17 @@ __global__ void __launch_bounds__(256) k_bin_count(ParticleBuf pb, long long n, 
 //   sum over cells c' of min(n_c', r)   (particles of lower rank)
 // + #{c' < c : n_c' > r}                (rank r in lower cells),
 // and, cell-major, sum over c' < c of n_c' + r; the particle's state moves
-// there.  Ranks are exact, so the slots are a permutation of the segment; a
-// slot outside it (inconsistent counts) is reported, not written.
+// there (move_vc = 0: all but the v and C planes -- inside the substep loop
+// the fused kernels never read them, they rewrite the v planes and rebuild
+// both on demand).  Ranks are exact, so the slots are a permutation of the
+// segment; a slot outside it (inconsistent counts) is reported, not written.
 template <int D, bool PAGED>
 __global__ void __launch_bounds__(256) k_bin_place(ParticleBuf src, ParticleBuf dst, long long n,
                                                    const unsigned long long* __restrict__ key,
                                                    const int* __restrict__ rank, const int* __restrict__ cell_count,
                                                    const int* __restrict__ seg_count,
                                                    const int* __restrict__ seg_start, MatSlots ms, int cell_major,
-                                                   unsigned* __restrict__ err, GridPages gp) {
+                                                   int move_vc, unsigned* __restrict__ err, GridPages gp) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const unsigned long long k = key[i];
@@ -149,7 +151,8 @@ __global__ void __launch_bounds__(256) k_bin_place(ParticleBuf src, ParticleBuf 
     }
     const long long j = (long long)seg_start[seg] + off;
 #pragma unroll
-    for (int p = 0; p < Planes<D>::COUNT; ++p) dst.s[p * dst.cap + j] = src.s[p * src.cap + i];
+    for (int p = 0; p < Planes<D>::COUNT; ++p)
+        if (move_vc || p < Planes<D>::V || p >= Planes<D>::F) dst.s[p * dst.cap + j] = src.s[p * src.cap + i];
     dst.grp[j] = src.grp[i];
     dst.id[j] = src.id[i];
 }
