@@ -499,17 +499,20 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // starts the asynchronous copy of chunk c's grid-velocity window into tv
-// (zero outside the grid), NT threads.  PAGED: through the page table (zero
-// for a block without a page), and the physical blocks of the window's 3^D
-// blocks (trash outside the scene) into s27 for the chunk's scatter.
-template <int D, int NT, bool PAGED>
-__device__ __forceinline__ void prefetch_velocity_tile(const FusedArgs& A, int c, float4* tv, int* s27) {
+// (zero outside the grid), NT threads, and keeps the chunk's record in
+// *s_ch for the chunk's pass.  PAGED: through the page table (zero for a
+// block without a page), and the physical blocks of the window's 3^D blocks
+// (trash outside the scene) into s27 for the chunk's scatter.
+template <int D, int NT, bool FIXED, bool PAGED>
+__device__ __forceinline__ void prefetch_velocity_tile(const FusedArgs& A, int c, float4* tv, int* s27,
+                                                       Chunk* s_ch) {
     constexpr int T = TileShape<D>::T;
     constexpr int S = BlockShape<D>::SHIFT;
     constexpr int M = BlockShape<D>::SIDE - 1;
     constexpr int SIDE = BlockShape<D>::SIDE;
     const Chunk ch = A.chunks[c];
-    const SceneParams& sc = A.scenes[ch.scene];
+    if (threadIdx.x == 0) *s_ch = ch;
+    const SceneParams& sc = chunk_scene<FIXED>(A, ch.scene);
     const float4* g = A.grid_vel + sc.node_off;
     if constexpr (PAGED) {
         if ((int)threadIdx.x < (D == 3 ? 27 : 9)) {
@@ -859,6 +862,7 @@ struct SpeedFlush {
 template <int D, int NT, bool FIXED = false, bool PAGED = false, class Body, class Post>
 __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][TileShape<D>::VN], int (&s27)[2][27],
                                            unsigned (&touched)[2], int (&s_cn)[2], Body body, Post post) {
+    __shared__ Chunk s_ch[2];  // the records of the current and the next chunk
     const int nch = *A.n_chunks;
     if (threadIdx.x == 0) {
         s_cn[0] = atomicAdd(A.cursor, 1);
@@ -867,24 +871,29 @@ __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][T
     __syncthreads();
     int cur = s_cn[0], nxt = s_cn[1];
     __syncthreads();  // s_cn is rewritten below
-    if (cur < nch) prefetch_velocity_tile<D, NT, PAGED>(A, cur, tv[0], s27[0]);
+    if (cur < nch) prefetch_velocity_tile<D, NT, FIXED, PAGED>(A, cur, tv[0], s27[0], &s_ch[0]);
     cp_async_commit();
     for (int k = 0; cur < nch; ++k) {
         const int b = k & 1;
-        if (nxt < nch) prefetch_velocity_tile<D, NT, PAGED>(A, nxt, tv[b ^ 1], s27[b ^ 1]);
+        if (nxt < nch) prefetch_velocity_tile<D, NT, FIXED, PAGED>(A, nxt, tv[b ^ 1], s27[b ^ 1], &s_ch[b ^ 1]);
         cp_async_commit();
+        // the chunk after next: thread 0 keeps the cursor's answer in a
+        // register and publishes it before barrier (2), so the atomic's round
+        // trip overlaps the chunk's pass
+        int after_next = 0;
         if (threadIdx.x == 0) {
-            s_cn[b] = atomicAdd(A.cursor, 1);  // the chunk after next
+            after_next = atomicAdd(A.cursor, 1);
             touched[b] = 0u;
         }
         cp_async_wait<1>();  // this thread's copies of the current window
-        __syncthreads();     // (1) everyone's; s_cn[b] and touched[b] published
-        const Chunk ch = A.chunks[cur];
+        __syncthreads();     // (1) everyone's; s_ch[b] and touched[b] published
+        const Chunk ch = s_ch[b];
         const int si = ch.scene;
         const SceneParams& sc = chunk_scene<FIXED>(A, si);
         const int o[3] = {ch.o[0], ch.o[1], ch.o[2]};
         body(ch, sc, o, tv[b], &touched[b], s27[b]);
-        __syncthreads();     // (2)
+        if (threadIdx.x == 0) s_cn[b] = after_next;
+        __syncthreads();     // (2) s_cn[b] published
         mark_touched<D>(touched[b], sc, o, A);
         post(si);
         cur = nxt;

@@ -152,7 +152,9 @@ MPM_HD void svd3(const float* F, float* U, float* s, float* V) {
                            F[2 * 3 + i] * F[2 * 3 + j];
 #pragma unroll
     for (int i = 0; i < 9; ++i) V[i] = (i % 4 == 0) ? 1.f : 0.f;
-#pragma unroll
+    // the sweep loop stays rolled: one copy of the three rotations keeps the
+    // fused kernels' code small (instruction-fetch stalls)
+#pragma unroll 1
     for (int sweep = 0; sweep < 4; ++sweep) {
         if (sweep >= 2 && jacobi_converged(S)) break;
         jacobi_rotate<0, 1>(S, V);
@@ -288,7 +290,7 @@ MPM_HD void kirchhoff_fcr3(const float* F, float mu, float lambda, float* tau) {
             S[i * 3 + j] = F[i * 3 + 0] * F[j * 3 + 0] + F[i * 3 + 1] * F[j * 3 + 1] + F[i * 3 + 2] * F[j * 3 + 2];
 #pragma unroll
     for (int i = 0; i < 9; ++i) U[i] = (i % 4 == 0) ? 1.f : 0.f;
-#pragma unroll
+#pragma unroll 1  // rolled, as in svd3
     for (int sweep = 0; sweep < 4; ++sweep) {
         if (sweep >= 2 && jacobi_converged(S)) break;
         jacobi_rotate<0, 1>(S, U);

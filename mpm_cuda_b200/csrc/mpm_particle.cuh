@@ -297,7 +297,9 @@ __device__ __forceinline__ void g2p_gather(const Stencil<D>& st, float inv_h, Fe
             G[a][b] = 0.f;
         }
     if constexpr (D == 3) {
-#pragma unroll
+        // both outer loops stay rolled (9 copies of the z row instead of 27):
+        // smaller code, fewer instruction-fetch stalls in the fused kernels
+#pragma unroll 1
         for (int ox = 0; ox < 3; ++ox) {
             float B00[3] = {0.f, 0.f, 0.f}, B10[3] = {0.f, 0.f, 0.f}, B20[3] = {0.f, 0.f, 0.f};
             float B01[3] = {0.f, 0.f, 0.f}, B02[3] = {0.f, 0.f, 0.f};
