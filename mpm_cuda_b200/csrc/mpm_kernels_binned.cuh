@@ -218,8 +218,12 @@ static __global__ void k_count_rebin(int* counter) { *counter += 1; }
 
 // ------------------------------------------------------ block activity --
 
-// marks global block gb as touched by P2G and appends it to the active list
+// marks global block gb as touched by P2G and appends it to the active list.
+// Most callers find the block marked already (every particle of a block marks
+// the same few blocks): a read at L2 first spares them the contended exchange;
+// a stale zero only costs the exchange, which decides.
 __device__ __forceinline__ void mark_block(unsigned* blk_flag, int* active, int* n_active, long long gb) {
+    if (__ldcg(&blk_flag[gb]) != 0u) return;
     if (atomicExch(&blk_flag[gb], 1u) == 0u) active[atomicAdd(n_active, 1)] = (int)gb;
 }
 
