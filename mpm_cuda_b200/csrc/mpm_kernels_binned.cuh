@@ -854,15 +854,16 @@ struct SpeedFlush {
 
 // Persistent loop of a CTA over a material's chunk list.  Chunks come from a
 // global cursor (chunk sizes vary); the index of the chunk after next and the
-// next chunk's velocity window are fetched while the current chunk is
-// processed, so the cursor atomic and the window's L2 round trips are off the
-// critical path.  body(ch, sc, o, tv, touched) runs with chunk ch's window in
-// tv; every thread of the CTA calls it; post(scene index) runs after the
-// body's barrier.  Two barriers per chunk: (1) window landed, the chunk after
-// next and the cleared touched word published; (2) body done (touched
-// complete, window free).  Shared words of parity b = k & 1 are rewritten two
-// chunks later, after both barriers of the chunk in between.  PAGED: the
-// window's physical blocks (s27) are fetched with the window.
+// next chunk's record and velocity window are fetched while the current chunk
+// is processed, so the cursor atomic and the L2 round trips of the record and
+// the window are off the critical path.  body(ch, sc, o, tv, touched) runs
+// with chunk ch's window in tv; every thread of the CTA calls it; post(scene
+// index) runs after the body's barrier.  Two barriers per chunk: (1) window
+// landed, the chunk's record and the cleared touched word published; (2) body
+// done (touched complete, window free), the index of the chunk after next
+// published.  Shared words of parity b = k & 1 are rewritten two chunks
+// later, after both barriers of the chunk in between.  PAGED: the window's
+// physical blocks (s27) are fetched with the window.
 template <int D, int NT, bool FIXED = false, bool PAGED = false, class Body, class Post>
 __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][TileShape<D>::VN], int (&s27)[2][27],
                                            unsigned (&touched)[2], int (&s_cn)[2], Body body, Post post) {
