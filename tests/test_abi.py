@@ -105,7 +105,7 @@ def test_kernel_config_table():
         assert lib.mpm_kernel_config_info(i, C.byref(ch), C.byref(mb), C.byref(rd)) == L.OK
         assert lib.mpm_kernel_config_scatter(i, C.byref(cm), C.byref(sg)) == L.OK
         assert ch.value in (64, 128, 256) and ch.value * mb.value <= 2048
-        assert rd.value in (1, 2, 4)
+        assert rd.value in (1, 2, 3, 4)
         assert cm.value in (0, 1) and sg.value in (0, 1)
         assert not (sg.value and not cm.value)  # the segmented scatter runs on cell-major chunks
         seen.add((ch.value, mb.value, rd.value, cm.value, sg.value))
