@@ -363,6 +363,9 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     const size_t grid_bytes = (size_t)grid_blocks_alloc() * 64 * sizeof(float4);
     if ((rc = alloc((void**)&grid_mom, grid_bytes, "grid_mom")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&grid_vel, grid_bytes, "grid_vel")) != MPM_OK) return rc;
+    // the fixed-scene dense kernels load their windows through vel_map; a
+    // driver without tensor maps leaves the run on the table-reading kernels
+    if (fixed_scene && !paged && encode_vel_map() != MPM_OK) fixed_scene = false;
     if ((rc = alloc((void**)&err_d, sizeof(unsigned), "err")) != MPM_OK) return rc;
     for (int p = 0; p < 2; ++p) {
         if ((rc = alloc((void**)&keys[p], cap * sizeof(unsigned long long), "sort keys")) != MPM_OK) return rc;
@@ -807,6 +810,36 @@ void Engine::enqueue_rebin(int from, bool in_loop) {
     sorted_order = true;
 }
 
+// Tensor map of the single scene's grid velocities in the linear layout:
+// float32 (component, x, y[, z]) with strides 16 B, 16 n0 B[, 16 n0 n1 B];
+// a box is one chunk window (4 x 8 x 8 x 8, or 4 x 12 x 12 in 2D), zero
+// outside the grid.  The encoder comes from the driver through the runtime,
+// so the library does not link the driver API.
+int Engine::encode_vel_map() {
+    using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+        cudaGetLastError();
+        return MPM_ERR_UNSUPPORTED;
+    }
+    const SceneParams& sc = scenes_h[0];
+    const cuuint32_t rank = dim == 3 ? 4 : 3;
+    const cuuint64_t dims[4] = {4, (cuuint64_t)sc.n[0], (cuuint64_t)sc.n[1], (cuuint64_t)sc.n[2]};
+    const cuuint64_t strides[3] = {16, 16ull * sc.n[0], 16ull * sc.n[0] * sc.n[1]};
+    const cuuint32_t box[4] = {4, (cuuint32_t)TileShape<3>::T, (cuuint32_t)TileShape<3>::T, (cuuint32_t)TileShape<3>::T};
+    const cuuint32_t box2[3] = {4, (cuuint32_t)TileShape<2>::T, (cuuint32_t)TileShape<2>::T};
+    const cuuint32_t elem[4] = {1, 1, 1, 1};
+    const CUresult r = reinterpret_cast<Encode>(fn)(
+        &vel_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, grid_vel + sc.node_off, dims, strides,
+        dim == 3 ? box : box2, elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? MPM_OK : MPM_ERR_UNSUPPORTED;
+}
+
 FusedArgs Engine::fused_args(int mat, bool bump) {
     FusedArgs A;
     A.chunks = chunks + mat * list_cap;
@@ -836,6 +869,7 @@ FusedArgs Engine::fused_args(int mat, bool bump) {
         if (g.type == mat && ++n_of_mat == 1) A.group = g;
     A.one_group = n_of_mat == 1 ? 1 : 0;
     A.pages = pages;
+    A.vel_map = vel_map;
     return A;
 }
 
@@ -869,7 +903,8 @@ void Engine::enqueue_grid_update() {
     const cudaError_t e = cudaLaunchKernelEx(&lc, k, grid_mom, grid_vel, (const int*)active, counters + CNT_ACTIVE,
                                              blk_flag, blk_epoch, (const int*)(counters + CNT_EPOCH),
                                              (const SceneParams*)scenes_d, n_scenes, counters + CNT_CURSOR, (int)kMats,
-                                             (unsigned*)(counters + CNT_UPDATE_DONE), scenes_h[0], pages, err_d);
+                                             (unsigned*)(counters + CNT_UPDATE_DONE), scenes_h[0],
+                                             vel_linear_mode() ? 1 : 0, pages, err_d);
     note_launch_status("k_grid_update_active", e);
 }
 
@@ -992,7 +1027,7 @@ int Engine::recover_vc() {
         auto k = dim == 3 ? (paged ? k_recover_vc<3, true> : k_recover_vc<3, false>)
                           : (paged ? k_recover_vc<2, true> : k_recover_vc<2, false>);
         k<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(buf(cur), n_particles, groups_d, scenes_d, grid_vel,
-                                                             pages);
+                                                             vel_lin_state ? 1 : 0, pages);
         MPM_CUDA_TRY(cudaGetLastError(), "v/C recovery launch");
     }
     vc_deferred = false;
@@ -1087,6 +1122,7 @@ int Engine::step(int n) {
                          "grid clear");
             grid_dirty = false;
         }
+        if (n > 0) vel_lin_state = false;  // the dense grid update writes the blocked layout
         if (opt.use_graph) {
             if (!graphs[cur][0]) {
                 cudaGraph_t g = nullptr;
@@ -1108,6 +1144,7 @@ int Engine::step(int n) {
             int rc = prologue();
             if (rc != MPM_OK) return rc;
         }
+        if (n > 0) vel_lin_state = false;  // read back by k_g2p_direct in the blocked layout
         if (opt.use_graph) {
             if (!graphs[cur][0]) {
                 cudaGraph_t g = nullptr;
@@ -1137,6 +1174,8 @@ int Engine::step(int n) {
             int rc = prologue();
             if (rc != MPM_OK) return rc;
         }
+        // (after the prologue, whose v/C recovery reads the previous layout)
+        if (n > 0) vel_lin_state = vel_linear_mode();
         const int run = opt.rebin_interval - 1;  // plain substeps between two re-binnings
         // set after every launched substep, so an early return below leaves it
         // describing the state the launched substeps produced
@@ -1353,9 +1392,24 @@ int Engine::set_state(int scene, const float* x, const float* v, const float* C,
 }
 
 // the scene's grid velocities in the dense blocked order (a paged block
-// without a page reads as zero)
+// without a page reads as zero; a grid in the linear layout is reordered)
 int Engine::download_grid(const SceneParams& sc, std::vector<float4>& blk) {
     blk.assign((size_t)sc.n_nodes, make_float4(0.f, 0.f, 0.f, 0.f));
+    if (!paged && vel_lin_state) {
+        const long long nl = (long long)sc.n[0] * sc.n[1] * (dim == 3 ? sc.n[2] : 1);
+        std::vector<float4> lin((size_t)nl);
+        MPM_CUDA_TRY(cudaMemcpy(lin.data(), grid_vel + sc.node_off, nl * sizeof(float4), cudaMemcpyDeviceToHost),
+                     "grid download");
+        const int side = dim == 3 ? 4 : 8, sh = dim == 3 ? 2 : 3;
+        for (int iz = 0; iz < (dim == 3 ? sc.n[2] : 1); ++iz)
+            for (int iy = 0; iy < sc.n[1]; ++iy)
+                for (int ix = 0; ix < sc.n[0]; ++ix) {
+                    const long long b = (ix >> sh) + (long long)sc.nb[0] * ((iy >> sh) + (long long)sc.nb[1] * (iz >> sh));
+                    const int in = (ix & (side - 1)) + side * ((iy & (side - 1)) + side * (iz & (side - 1)));
+                    blk[(size_t)(b * 64 + in)] = lin[(size_t)(ix + (long long)sc.n[0] * (iy + (long long)sc.n[1] * iz))];
+                }
+        return MPM_OK;
+    }
     if (!paged) {
         MPM_CUDA_TRY(cudaMemcpy(blk.data(), grid_vel + sc.node_off, sc.n_nodes * sizeof(float4), cudaMemcpyDeviceToHost),
                      "grid download");
@@ -1562,6 +1616,7 @@ int Engine::profile_stages(int n, float* out_ms, int n_out, int* n_written) {
             int rc = prologue();
             if (rc != MPM_OK) return rc;
         }
+        if (n > 0) vel_lin_state = vel_linear_mode();
         // re-binnings at the handle's interval, as in step(); reported per
         // re-binning, the other stages per substep
         int n_rebin = 0;
@@ -1598,6 +1653,7 @@ int Engine::profile_stages(int n, float* out_ms, int n_out, int* n_written) {
             int rc = prologue();
             if (rc != MPM_OK) return rc;
         }
+        if (n > 0) vel_lin_state = false;  // read back by k_g2p_direct in the blocked layout
         const ParticleBuf pb = buf(cur);
         for (int it = 0; it < n; ++it) {
             cudaEventRecord(ev[0], stream);
@@ -1627,6 +1683,7 @@ int Engine::profile_stages(int n, float* out_ms, int n_out, int* n_written) {
             cudaMemsetAsync(grid_mom, 0, (size_t)total_blocks * 64 * sizeof(float4), stream);
             grid_dirty = false;
         }
+        if (n > 0) vel_lin_state = false;  // the dense grid update writes the blocked layout
         for (int it = 0; it < n; ++it) {
             cudaEventRecord(ev[0], stream);
             if (dim == 3) {

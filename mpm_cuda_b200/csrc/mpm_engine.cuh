@@ -1,6 +1,7 @@
 // Engine behind the C-ABI handle: device memory, stream, substep graphs.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap
 #include <cuda_runtime.h>
 
 #include <string>
@@ -100,6 +101,14 @@ struct Engine {
     // fused kernels deferred them (k_recover_vc rebuilds both)
     bool vc_deferred = false;
     bool defer_vc_now() const;
+    // the single-scene dense fused path keeps grid velocities in the linear
+    // layout and loads its windows as boxes of vel_map (encoded at creation);
+    // vel_lin_state: the layout of what grid_vel holds now (the last grid
+    // update's), for the readers outside the fused pass
+    CUtensorMap vel_map{};
+    bool vel_lin_state = false;
+    bool vel_linear_mode() const { return fixed_scene && !paged && fused(); }
+    int encode_vel_map();
     int recover_vc();
     // learned stress (MPM_STRESS_SURROGATE): the network, the version of its
     // weights the graphs were captured with, per-material persistent CTAs and

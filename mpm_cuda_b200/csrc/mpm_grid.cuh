@@ -128,6 +128,16 @@ __device__ __forceinline__ float4 grid_read(const float4* g, const SceneParams& 
     return g[b * 64 + in];
 }
 
+// Linear velocity layout.  The single-scene dense fused path keeps grid
+// velocities x-fastest row by row (node (ix, iy, iz) at node_off + ix +
+// n0 (iy + n1 iz)), so the fused kernel's window is one box of a tensor that
+// the copy engine (TMA) loads whole; momentum keeps the blocked layout.  The
+// scene's linear nodes fit in its blocked range (n0 n1 n2 <= 64 blocks).
+template <int D>
+__device__ __forceinline__ long long lin_node(const SceneParams& sc, int ix, int iy, int iz) {
+    return sc.node_off + ix + (long long)sc.n[0] * (iy + (D == 3 ? (long long)sc.n[1] * iz : 0LL));
+}
+
 // scene owning global block `b` (binary search over block_off)
 __device__ __forceinline__ int scene_of_block(const SceneParams* scenes, int n_scenes, long long b) {
     int lo = 0, hi = n_scenes - 1;

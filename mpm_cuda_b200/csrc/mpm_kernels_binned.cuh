@@ -17,6 +17,8 @@
 // memory directly, so results never depend on how stale the binning is.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap
+
 #include "mpm_config.cuh"
 #include "mpm_grid.cuh"
 #include "mpm_kernels_direct.cuh"
@@ -35,9 +37,10 @@ struct Chunk {
     int o[3];   // window origin: the home block's first node minus one per axis
 };
 
-// Tile layout.  3D: window 8^3, stored densely (strides 1, 8, 64) with x
-// XOR-ed by 4 on odd y, so the 8 lanes of an LDS.128 phase (cells x 0..3,
-// y 0..1) read 8 distinct 16-byte bank groups.  2D: window 12^2, stride 12.
+// Tile layout.  3D: window 8^3, stored densely (strides 1, 8, 64); 2D:
+// window 12^2, stride 12 -- the layout a tensor-map box load writes (an XOR
+// swizzle of x on odd y, against bank conflicts of the gather, measured no
+// faster).
 template <int D>
 struct TileShape;
 
@@ -47,7 +50,7 @@ struct TileShape<3> {
     static constexpr int T = 8;
     static constexpr int N = 512;
     static constexpr int VY = 8, VZ = 64, VN = 512;
-    static constexpr bool SWIZZLE = true;
+    static constexpr bool SWIZZLE = false;
 };
 
 template <>
@@ -377,9 +380,11 @@ __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.lau
 // active-block count and the fused kernels' chunk cursors for the next pass
 // (every CTA has read the count before it counts itself done).
 // FIXED: the one scene of a fixed-dt run comes from the kernel parameters
-// (fixed_scene), as in the fused kernel.  PAGED: a block's nodes through its
-// physical block, and every neighbour of an updated block gets a physical
-// block (the next P2G reaches at most one block further).
+// (fixed_scene), as in the fused kernel.  vel_linear (dense grid): velocities
+// in the linear layout (lin_node; nodes of a block beyond the grid's edge are
+// not written).  PAGED: a block's nodes through its physical block, and every
+// neighbour of an updated block gets a physical block (the next P2G reaches
+// at most one block further).
 template <int D, bool FIXED, bool PAGED>
 __global__ void __launch_bounds__(256) k_grid_update_active(float4* __restrict__ grid_mom, float4* __restrict__ grid_vel,
                                                             const int* __restrict__ active, int* __restrict__ n_active,
@@ -388,7 +393,7 @@ __global__ void __launch_bounds__(256) k_grid_update_active(float4* __restrict__
                                                             const SceneParams* __restrict__ scenes, int n_scenes,
                                                             int* __restrict__ cursors, int n_cursors,
                                                             unsigned* __restrict__ done, SceneParams fixed_scene,
-                                                            GridPages gp, unsigned* __restrict__ err_word) {
+                                                            int vel_linear, GridPages gp, unsigned* __restrict__ err_word) {
     pdl_wait();
     const int na = *n_active;
     const int ep = *epoch;
@@ -405,7 +410,9 @@ __global__ void __launch_bounds__(256) k_grid_update_active(float4* __restrict__
         if (!PAGED || pb < gp.trash) {
             const long long gi = pb * 64 + lane;
             const float4 g = grid_mom[gi];
-            grid_vel[gi] = grid_node_update<D>(g, sc, ix, iy, iz);
+            const float4 v = grid_node_update<D>(g, sc, ix, iy, iz);
+            if (PAGED || !vel_linear) grid_vel[gi] = v;
+            else if (ix < sc.n[0] && iy < sc.n[1] && (D == 2 || iz < sc.n[2])) grid_vel[lin_node<D>(sc, ix, iy, iz)] = v;
             grid_mom[gi] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
         if constexpr (PAGED) {
@@ -464,6 +471,11 @@ struct FusedArgs {
     int one_group;
     GroupParams group;
     GridPages pages;  // paged grid (the PAGED kernels)
+    // FIXED dense kernels: grid_vel in the linear layout as a tensor of
+    // (component, x, y[, z]) float32, box = one chunk window; the kernels take
+    // FusedArgs as a __grid_constant__ parameter, so the copy engine reads the
+    // map from the parameter space
+    CUtensorMap vel_map;
 };
 
 // the group record of particle i of a fused launch
@@ -502,6 +514,52 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// ---- window by tensor-map box load (FIXED dense kernels)
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Waits for phase `parity` of the barrier; false after ~2 s (2^32 cycles)
+// without completion, which only a broken copy can cause
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    const unsigned a = smem_addr(bar);
+    const long long t0 = clock64();
+    for (;;) {
+        unsigned ok;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(ok) : "r"(a), "r"(parity) : "memory");
+        if (ok) return true;
+        if (clock64() - t0 > (1LL << 32)) return false;
+    }
+}
+
+// One thread: the window of origin o as one box of the velocity tensor map
+// into tv (zero outside the grid), completing on `bar`.  The box starts on a
+// component index of 0, so its innermost coordinate is 16-byte aligned; the
+// x, y, z coordinates may be -1 or reach past the grid (zero fill).
+template <int D>
+__device__ __forceinline__ void tma_window(const CUtensorMap* map, float4* tv, unsigned long long* bar, const int* o) {
+    constexpr unsigned bytes = TileShape<D>::VN * sizeof(float4);
+    const unsigned dst = smem_addr(tv), mb = smem_addr(bar);
+    // the window's previous contents were read through the generic proxy
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mb), "r"(bytes) : "memory");
+    if constexpr (D == 3) {
+        asm volatile(
+            "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];\n"
+            ::"r"(dst), "l"(reinterpret_cast<unsigned long long>(map)), "r"(0), "r"(o[0]), "r"(o[1]), "r"(o[2]), "r"(mb)
+            : "memory");
+    } else {
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n"
+            ::"r"(dst), "l"(reinterpret_cast<unsigned long long>(map)), "r"(0), "r"(o[0]), "r"(o[1]), "r"(mb)
+            : "memory");
+    }
+}
+
 // starts the asynchronous copy of chunk c's grid-velocity window into tv
 // (zero outside the grid), NT threads, and keeps the chunk's record in
 // *s_ch for the chunk's pass.  PAGED: through the page table (zero for a
@@ -509,11 +567,20 @@ __device__ __forceinline__ void cp_async_wait() {
 // (trash outside the scene) into s27 for the chunk's scatter.
 template <int D, int NT, bool FIXED, bool PAGED>
 __device__ __forceinline__ void prefetch_velocity_tile(const FusedArgs& A, int c, float4* tv, int* s27,
-                                                       Chunk* s_ch) {
+                                                       Chunk* s_ch, unsigned long long* bar) {
     constexpr int T = TileShape<D>::T;
     constexpr int S = BlockShape<D>::SHIFT;
     constexpr int M = BlockShape<D>::SIDE - 1;
     constexpr int SIDE = BlockShape<D>::SIDE;
+    if constexpr (FIXED && !PAGED) {
+        // one box load of the linear velocity tensor, issued by one thread
+        if (threadIdx.x == 0) {
+            const Chunk ch = A.chunks[c];
+            *s_ch = ch;
+            tma_window<D>(&A.vel_map, tv, bar, ch.o);
+        }
+        return;
+    }
     const Chunk ch = A.chunks[c];
     if (threadIdx.x == 0) *s_ch = ch;
     const SceneParams& sc = chunk_scene<FIXED>(A, ch.scene);
@@ -562,8 +629,9 @@ __device__ __forceinline__ bool in_window(const int* base, const int* o) {
 }
 
 // G2P of one particle from the window, or from global memory for a particle
-// that drifted out of it since the last re-binning
-template <int D, bool PAGED = false>
+// that drifted out of it since the last re-binning (LIN: grid_vel in the
+// linear layout)
+template <int D, bool PAGED = false, bool LIN = false>
 __device__ __forceinline__ void g2p_window(const Stencil<D>& st, const int* o, const float4* tv, const SceneParams& sc,
                                            const FusedArgs& A, G2PAcc<D>& acc) {
     if (in_window<D>(st.base, o)) {
@@ -576,6 +644,11 @@ __device__ __forceinline__ void g2p_window(const Stencil<D>& st, const int* o, c
         g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) {
             return grid_read<D, true>(A.grid_vel, sc, A.pages, st.base[0] + ox, st.base[1] + oy,
                                       D == 3 ? st.base[2] + oz : 0);
+        }, acc);
+    } else if constexpr (LIN) {
+        atomicAdd(A.fallback, 1u);
+        g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) {
+            return A.grid_vel[lin_node<D>(sc, st.base[0] + ox, st.base[1] + oy, D == 3 ? st.base[2] + oz : 0)];
         }, acc);
     } else {
         atomicAdd(A.fallback, 1u);
@@ -867,20 +940,30 @@ struct SpeedFlush {
 template <int D, int NT, bool FIXED = false, bool PAGED = false, class Body, class Post>
 __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][TileShape<D>::VN], int (&s27)[2][27],
                                            unsigned (&touched)[2], int (&s_cn)[2], Body body, Post post) {
+    constexpr bool TMA = FIXED && !PAGED;  // windows by tensor-map box loads
     __shared__ Chunk s_ch[2];  // the records of the current and the next chunk
+    // TMA: completion of window b's loads; window b's n-th load completes
+    // phase n, so chunk k waits for parity (k >> 1) & 1 of barrier k & 1
+    __shared__ __align__(8) unsigned long long s_bar[2];
     const int nch = *A.n_chunks;
     if (threadIdx.x == 0) {
         s_cn[0] = atomicAdd(A.cursor, 1);
         s_cn[1] = atomicAdd(A.cursor, 1);
+        if constexpr (TMA) {
+            mbar_init(&s_bar[0]);
+            mbar_init(&s_bar[1]);
+            asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        }
     }
     __syncthreads();
     int cur = s_cn[0], nxt = s_cn[1];
     __syncthreads();  // s_cn is rewritten below
-    if (cur < nch) prefetch_velocity_tile<D, NT, FIXED, PAGED>(A, cur, tv[0], s27[0], &s_ch[0]);
+    if (cur < nch) prefetch_velocity_tile<D, NT, FIXED, PAGED>(A, cur, tv[0], s27[0], &s_ch[0], &s_bar[0]);
     cp_async_commit();
     for (int k = 0; cur < nch; ++k) {
         const int b = k & 1;
-        if (nxt < nch) prefetch_velocity_tile<D, NT, FIXED, PAGED>(A, nxt, tv[b ^ 1], s27[b ^ 1], &s_ch[b ^ 1]);
+        if (nxt < nch)
+            prefetch_velocity_tile<D, NT, FIXED, PAGED>(A, nxt, tv[b ^ 1], s27[b ^ 1], &s_ch[b ^ 1], &s_bar[b ^ 1]);
         cp_async_commit();
         // the chunk after next: thread 0 keeps the cursor's answer in a
         // register and publishes it before barrier (2), so the atomic's round
@@ -891,7 +974,16 @@ __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][T
             touched[b] = 0u;
         }
         cp_async_wait<1>();  // this thread's copies of the current window
-        __syncthreads();     // (1) everyone's; s_ch[b] and touched[b] published
+        // (1) everyone's copies landed; s_ch[b] and touched[b] published
+        if constexpr (TMA) {
+            const bool ok = mbar_wait(&s_bar[b], (unsigned)(k >> 1) & 1u);
+            if (__syncthreads_or(!ok)) {  // a window that never arrived: report it and stop
+                if (threadIdx.x == 0) atomicOr(A.err_word, ERR_TIMEOUT);
+                break;
+            }
+        } else {
+            __syncthreads();
+        }
         const Chunk ch = s_ch[b];
         const int si = ch.scene;
         const SceneParams& sc = chunk_scene<FIXED>(A, si);
@@ -917,11 +1009,11 @@ __device__ __forceinline__ void chunk_loop(const FusedArgs& A, float4 (&tv)[2][T
 // (SCATTER_SEGMENTED, staging buffer in dynamic shared memory).  FIXED: the
 // scene comes from A.scene (one scene, dt fixed for the run).
 template <int D, int MAT, int CHUNK, int MINB, bool FIXED, int SCATTER, bool PAGED>
-__global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs A) {
+__global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, const __grid_constant__ FusedArgs A) {
     using P = Planes<D>;
     using TS = TileShape<D>;
     static_assert(!(PAGED && SCATTER == SCATTER_SEGMENTED), "the segmented scatter addresses a dense grid");
-    __shared__ __align__(16) float4 tv[2][TS::VN];  // grid velocity windows (double-buffered)
+    __shared__ __align__(128) float4 tv[2][TS::VN];  // grid velocity windows (double-buffered; box-load targets)
     __shared__ int s27[2][27];                      // PAGED: the windows' physical blocks
     __shared__ unsigned touched[2];                 // 3^D neighbour-block bits
     __shared__ int s_cn[2];
@@ -959,7 +1051,7 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
                 Stencil<D> st;
                 if (make_stencil<D>(x, sc, st, err)) {
                     G2PAcc<D> acc;
-                    g2p_window<D, PAGED>(st, o, w, sc, A, acc);
+                    g2p_window<D, PAGED, FIXED && !PAGED>(st, o, w, sc, A, acc);
                     // loaded after the gather, its register peak
                     const GroupParams g = particle_group<FIXED>(A, pb, i);
                     float F[D * D], Cn[D * D], v[D], aux;
@@ -988,12 +1080,14 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g(ParticleBuf pb, FusedArgs
 // v and C of the last substep for particles whose fused pass deferred them:
 // the v planes hold the position the pass's G2P used, and grid_vel still holds
 // the velocities it gathered (the next grid update has not run), so the same
-// gather gives the same v and C = 4/h B.  A particle whose stencil left the
-// grid (the pass reported it) keeps its planes.
+// gather gives the same v and C = 4/h B (vel_linear: grid_vel in the linear
+// layout).  A particle whose stencil left the grid (the pass reported it)
+// keeps its planes.
 template <int D, bool PAGED>
 __global__ void __launch_bounds__(256) k_recover_vc(ParticleBuf pb, long long n, const GroupParams* __restrict__ groups,
                                                     const SceneParams* __restrict__ scenes,
-                                                    const float4* __restrict__ grid_vel, GridPages gp) {
+                                                    const float4* __restrict__ grid_vel, int vel_linear,
+                                                    GridPages gp) {
     using P = Planes<D>;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -1010,6 +1104,10 @@ __global__ void __launch_bounds__(256) k_recover_vc(ParticleBuf pb, long long n,
     if constexpr (PAGED) {
         g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) {
             return grid_read<D, true>(grid_vel, sc, gp, st.base[0] + ox, st.base[1] + oy, D == 3 ? st.base[2] + oz : 0);
+        }, acc);
+    } else if (vel_linear) {
+        g2p_gather<D>(st, sc.inv_h, [&](int ox, int oy, int oz) {
+            return grid_vel[lin_node<D>(sc, st.base[0] + ox, st.base[1] + oy, D == 3 ? st.base[2] + oz : 0)];
         }, acc);
     } else {
         const StencilIndex<D> ix(sc, st.base);

@@ -36,13 +36,14 @@ struct SurArgs {
 };
 
 template <int CHUNK, int MINB, bool FIXED, bool PAGED>
-__global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, FusedArgs A, SurArgs SA) {
+__global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, const __grid_constant__ FusedArgs A,
+                                                            SurArgs SA) {
     constexpr int D = 3;
     constexpr int MAT = JELLO;
     using TS = TileShape<D>;
     static_assert(CHUNK % 32 == 0, "whole warps");
     constexpr int XS = kSurRowStride, SS = kSurStashStride;
-    __shared__ __align__(16) float4 tv[2][TS::VN];  // grid velocity windows (double-buffered)
+    __shared__ __align__(128) float4 tv[2][TS::VN];  // grid velocity windows (double-buffered; box-load targets)
     __shared__ int s27[2][27];                      // PAGED: the windows' physical blocks
     __shared__ __align__(16) mlp::Forward W;        // network weights
     extern __shared__ float sxy[];                  // CHUNK network rows (inputs, then outputs), CHUNK stash rows
@@ -87,7 +88,7 @@ __global__ void __launch_bounds__(CHUNK, MINB) k_g2p2g_sur(ParticleBuf pb, Fused
                 Stencil<D> st;
                 if (make_stencil<D>(x, sc, st, err)) {
                     G2PAcc<D> acc;
-                    g2p_window<D, PAGED>(st, o, w, sc, A, acc);
+                    g2p_window<D, PAGED, FIXED && !PAGED>(st, o, w, sc, A, acc);
                     const GroupParams g = A.groups[gi];
                     float F[D * D], Cn[D * D], v[D], aux;
                     err |= update_and_store<D, MAT>(acc, sc, g, S, cap, i, x, v, Cn, F, aux, nullptr,
