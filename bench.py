@@ -277,6 +277,8 @@ def surrogate_leg(args, sim, scenes, stream, flush, plain_ms_per_step: float):
     try:
         with Simulation(timed, device=sim.device, kernel_config=sim.kernel_config()) as s2:
             s2.set_stress_mode(L.STRESS_SURROGATE, sur)
+            if args.kernel_config < 0:
+                s2.autotune()  # the launch configuration for the network kernel
             s2.step(args.warmup)
             s2.synchronize()
             t_ms = time_substeps(s2, torch.cuda.ExternalStream(s2.stream_ptr(), device=sim.device), flush,

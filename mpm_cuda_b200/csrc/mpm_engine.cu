@@ -503,10 +503,11 @@ void Engine::set_config(int ci) {
     grid_dirty = true;  // chunk lists depend on the chunk size
 }
 
-// CTA size of the learned-stress kernel: 128 threads when the chunk holds a
-// multiple of 128 particles (its shared rows then allow 16 warps per SM),
-// else the chunk's 64; it takes chunk_particles() / that many rounds
-int Engine::sur_chunk() const { return chunk_particles() % 128 == 0 ? 128 : 64; }
+// CTA size of the learned-stress kernel: 128 threads when the chunk holds at
+// least 128 particles (its shared rows then allow 16 warps per SM; 64-thread
+// CTAs measured slower), else 64; it takes ceil(chunk_particles() / that)
+// rounds, the last one partly idle when the chunk is not a multiple of it
+int Engine::sur_chunk() const { return chunk_particles() >= 128 ? 128 : 64; }
 
 void Engine::sur_occupancy() {
     for (int mat = 0; mat < kMats; ++mat) {
@@ -654,7 +655,9 @@ int Engine::autotune(int steps, float* best_ms) {
     int mats = 0;
     for (int m = 0; m < kMats; ++m) mats |= mat_present[m] ? (1 << m) : 0;
     std::lock_guard<std::mutex> lk(tune_mutex());
-    tune_cache()[TuneKey{device, dim, mats, n_particles, total_blocks, paged}] = best;
+    // the cache serves handle creation, which starts on the plain stress: a
+    // choice timed with the learned stress is not kept for it
+    if (!sur) tune_cache()[TuneKey{device, dim, mats, n_particles, total_blocks, paged}] = best;
     return MPM_OK;
 }
 
@@ -918,7 +921,7 @@ void Engine::enqueue_g2p2g(int parity) {
             const SurArgs SA{&sur->weights->f, sur->meta, sur_counts};
             const int ch = sur_chunk();
             FusedArgs As = A;
-            As.rounds = chunk_particles() / ch;
+            As.rounds = (chunk_particles() + ch - 1) / ch;
             cudaLaunchAttribute attr;
             const cudaLaunchConfig_t lc = pdl_config(sur_ctas[mat], ch, sur_dyn_smem(ch), stream, &attr);
             const cudaError_t e = cudaLaunchKernelEx(&lc, sur_fn(ch, fixed_scene, paged), buf(parity), As, SA);
