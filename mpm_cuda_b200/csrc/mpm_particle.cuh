@@ -385,6 +385,11 @@ __device__ __forceinline__ void g2p_gather(const Stencil<D>& st, float inv_h, Fe
 // parts precomputed per stencil row.  Node value for component c:
 //   w (alpha_c + sum_b beta_cb o_b) + sum_b A'_cb g_b(o),
 // alpha = m v - h (m C) fx, beta = h m C, A' = A / h, g_b = dw_b prod_{a!=b} w_a.
+// In 3D, with P = wx wy per (ox, oy) row, the value factors over z as
+//   wz (P (lin_c + oz beta_c2) + K_c) + dwz P A'_c2,
+// lin_c = alpha_c + ox beta_c0 + oy beta_c1, K_c = A'_c0 dwx wy + A'_c1 wx dwy:
+// per row U_c = P lin_c + K_c, V_c = P beta_c2, W_c = P A'_c2, then per node
+// two operations a component (offsets 0, 1, 2 as no-op, add, fma).
 // emit(ox, oy, oz, float4(momentum, mass)) receives each node's value.
 template <int D, class Emit>
 __device__ __forceinline__ void p2g_scatter(const Stencil<D>& st, const P2GSource<D>& src, float h, float inv_h,
@@ -402,29 +407,30 @@ __device__ __forceinline__ void p2g_scatter(const Stencil<D>& st, const P2GSourc
         alpha[c] = a0;
     }
     if constexpr (D == 3) {
+        // x + k b for a stencil offset k = 0, 1, 2 without a multiply by 0 or 1
+        auto off = [](float x, float b, int k) { return k == 0 ? x : (k == 1 ? x + b : fmaf(2.f, b, x)); };
 #pragma unroll
         for (int ox = 0; ox < 3; ++ox)
 #pragma unroll
             for (int oy = 0; oy < 3; ++oy) {
                 const float wx = st.w(0, ox), wy = st.w(1, oy);
                 const float P = wx * wy, Qx = st.dw(0, ox) * wy, Qy = wx * st.dw(1, oy);
-                float lin[3], K[3];
+                const float Pm = P * src.m;
+                float U[3], V[3], W[3];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    lin[c] = fmaf(beta[c][1], (float)oy, fmaf(beta[c][0], (float)ox, alpha[c]));
-                    K[c] = fmaf(Ap[c][1], Qy, Ap[c][0] * Qx);
+                    const float lin = off(off(alpha[c], beta[c][0], ox), beta[c][1], oy);
+                    U[c] = fmaf(P, lin, fmaf(Ap[c][1], Qy, Ap[c][0] * Qx));
+                    V[c] = P * beta[c][2];
+                    W[c] = P * Ap[c][2];
                 }
 #pragma unroll
                 for (int oz = 0; oz < 3; ++oz) {
-                    const float wz = st.w(2, oz);
-                    const float w = P * wz, Pdz = P * st.dw(2, oz);
+                    const float wz = st.w(2, oz), dz = st.dw(2, oz);
                     float out[3];
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        const float t = fmaf(beta[c][2], (float)oz, lin[c]);
-                        out[c] = fmaf(Pdz, Ap[c][2], fmaf(w, t, wz * K[c]));
-                    }
-                    emit(ox, oy, oz, make_float4(out[0], out[1], out[2], w * src.m));
+                    for (int c = 0; c < 3; ++c) out[c] = fmaf(wz, off(U[c], V[c], oz), dz * W[c]);
+                    emit(ox, oy, oz, make_float4(out[0], out[1], out[2], Pm * wz));
                 }
             }
     } else {
