@@ -306,6 +306,26 @@ def test_switching_modes_keeps_state(gpu):
     compare(got, orc.state(), {"x": 5e-6, "v": 1e-3, "C": 1e-3, "F": 5e-5, "aux": 5e-5})
 
 
+def test_grid_read_back_follows_the_velocity_layout(gpu):
+    # a single-scene dense run keeps grid velocities in the linear layout; a
+    # change of P2G path before the next substep leaves them so, and the grid
+    # read-back must still see the same values
+    sc = blob_scene(3, "jello", seed=93)
+    with Simulation([sc]) as sim:
+        sim.step(5)
+        m1, v1 = sim.get_grid(0)
+        sim.set_p2g_mode(L.P2G_DETERMINISTIC)
+        m2, v2 = sim.get_grid(0)
+        assert np.array_equal(v1, v2)
+        sim.step(1)  # the deterministic path's grid update writes the blocked layout
+        _, v3 = sim.get_grid(0)
+        assert np.abs(v3).max() > 0
+    with Simulation([sc, blob_scene(3, "jello", seed=94)]) as batch:  # two scenes: blocked layout
+        batch.step(5)
+        _, vb = batch.get_grid(0)
+    assert np.allclose(v1, vb, rtol=1e-4, atol=1e-6 * np.abs(vb).max())
+
+
 def test_set_state_mid_run_binned(gpu):
     sc = blob_scene(3, "jello", seed=92)
     with Simulation([sc], rebin_interval=5) as sim:
