@@ -306,6 +306,30 @@ def test_switching_modes_keeps_state(gpu):
     compare(got, orc.state(), {"x": 5e-6, "v": 1e-3, "C": 1e-3, "F": 5e-5, "aux": 5e-5})
 
 
+@pytest.mark.parametrize("d,n", [(3, 30), (2, 44)])
+def test_grid_not_a_multiple_of_the_block_near_its_upper_edge(gpu, d, n):
+    # the last block row reaches past the grid; windows near the upper edge
+    # load nodes outside it (zero), and the linear velocity layout of a
+    # single-scene run must not let the padding nodes of one row spill into
+    # the next
+    mat = MATS["jello"]
+    h = 1.0 / n
+    x, v, C, F, aux = S.perturbed_blob(d, mat, n_grid=n, h=h, ppc=2, radius_cells=3.5, seed=95,
+                                       center=np.full(d, (n - 8.5) * h))
+    g = group_from_arrays(mat, h, 2, x, v, C, F, aux)
+    sc = Scene(dim=d, n=(n,) * d, h=h, dt=1e-4, groups=[g], bc_type=L.BC_SLIP, bc_lo=3, bc_hi=3,
+               gravity=(0.0, -9.8, 0.0)[:d] if d == 3 else (0.0, -9.8))
+    orc = oracle_for(sc)
+    assert orc.step(6) == 0
+    ref = orc.state()
+    with Simulation([sc], rebin_interval=3) as sim:
+        sim.step(6)
+        compare(sim.get_state(0), ref, {"x": 5e-6, "v": 6e-4, "C": 6e-4, "F": 4e-5, "aux": 4e-5})
+    with Simulation([sc, blob_scene(d, "water", seed=96)], rebin_interval=3) as sim:  # blocked layout
+        sim.step(6)
+        compare(sim.get_state(0), ref, {"x": 5e-6, "v": 6e-4, "C": 6e-4, "F": 4e-5, "aux": 4e-5})
+
+
 def test_grid_read_back_follows_the_velocity_layout(gpu):
     # a single-scene dense run keeps grid velocities in the linear layout; a
     # change of P2G path before the next substep leaves them so, and the grid
