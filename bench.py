@@ -153,6 +153,19 @@ def measured_traffic(workload: str, kernel: str):
     return None
 
 
+def measured_counter(workload: str, kernel: str, metric: str):
+    """A per-particle counter of `kernel` on `workload` from the committed ncu
+    summaries (profiles/fused_counters.txt), or None without a capture."""
+    path = os.path.join(ROOT, "profiles", "fused_counters.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        f = line.split()
+        if len(f) >= 4 and not line.startswith("#") and f[:3] == [workload, kernel, metric]:
+            return float(f[3])
+    return None
+
+
 def state_bytes_per_particle(scenes):
     """Algorithmic bytes of one particle's state, FP32: x v C F for solids
     (+ det Fp for snow), x v C J for water."""
@@ -384,6 +397,27 @@ def run_ours(args, rank, world, local_rank, dist):
                 "substep_algorithmic_bytes": int(sub_bytes),
                 "substep_achieved": round(sub_bytes / (t_max_s / args.steps) / 1e9, 1),
                 "substep_frac": round(sub_bytes / (t_max_s / args.steps) / 1e9 / peak, 4)}
+    if args.mode == "binned":
+        # the two other ceilings of the fused kernel, beside HBM: its FP32 rate
+        # against the SMs' non-tensor FP32 peak at the sampled clock, and its
+        # node reductions (27 per particle in 3D, 9 in 2D)
+        fused_s = stages[stage_names.index("g2p2g")] * 1e-3
+        props = torch.cuda.get_device_properties(local_rank)
+        mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 0.0
+        flops = measured_counter(args.workload, "g2p2g", "fp32_flops_per_particle")
+        if flops is not None and mhz:
+            fp32_peak = props.multi_processor_count * 128 * 2 * mhz * 1e6 / 1e12
+            achieved_tf = flops * n_part / fused_s / 1e12
+            roofline["fp32"] = {"flops_per_particle": flops, "achieved": round(achieved_tf, 2),
+                                "peak": round(fp32_peak, 1), "unit": "TFLOP/s",
+                                "frac": round(achieved_tf / fp32_peak, 4),
+                                "source": "profiles/fused_counters.txt (ncu FFMA x2 + FMUL + FADD per particle); "
+                                          "peak = SMs x 128 FP32 lanes x 2 x median SM clock"}
+        per = 27 if scenes[0].dim == 3 else 9
+        roofline["reductions"] = {"per_particle": per, "achieved": round(per * n_part / fused_s / 1e9, 1),
+                                  "unit": "G node reductions/s (red.global.add.v4.f32)",
+                                  "l2_requests_per_particle": measured_counter(args.workload, "g2p2g",
+                                                                               "l2_red_requests_per_particle")}
 
     # end to end through the public API: every substep's positions reach host
     # memory inside the timed region.  Pipelined: two substeps are in flight
