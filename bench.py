@@ -411,7 +411,8 @@ def run_ours(args, rank, world, local_rank, dist):
             roofline["fp32"] = {"flops_per_particle": flops, "achieved": round(achieved_tf, 2),
                                 "peak": round(fp32_peak, 1), "unit": "TFLOP/s",
                                 "frac": round(achieved_tf / fp32_peak, 4),
-                                "source": "profiles/fused_counters.txt (ncu FFMA x2 + FMUL + FADD per particle); "
+                                "source": "profiles/fused_counters.txt (ncu FFMA x2 + FMUL + FADD + FFMA2 x4 "
+                                          "+ FMUL2 x2 + FADD2 x2 per particle); "
                                           "peak = SMs x 128 FP32 lanes x 2 x median SM clock"}
         per = 27 if scenes[0].dim == 3 else 9
         roofline["reductions"] = {"per_particle": per, "achieved": round(per * n_part / fused_s / 1e9, 1),

@@ -297,51 +297,66 @@ __device__ __forceinline__ void g2p_gather(const Stencil<D>& st, float inv_h, Fe
             G[a][b] = 0.f;
         }
     if constexpr (D == 3) {
+        // Components x and y as one pair on the paired FP32 instructions of
+        // sm_100 (FFMA2: two independent lanes per instruction, each rounded
+        // like fmaf), z scalar.  A "3-vector" below is a (float2 xy, float z).
+        struct V3 {
+            float2 xy;
+            float z;
+        };
+        auto zero = [] { return V3{make_float2(0.f, 0.f), 0.f}; };
+        // acc + s * x, per component
+        auto fma3 = [](float s, const V3& x, const V3& acc) {
+            return V3{__ffma2_rn(make_float2(s, s), x.xy, acc.xy), fmaf(s, x.z, acc.z)};
+        };
+        V3 vs = zero(), Sv[3] = {zero(), zero(), zero()}, Gv[3] = {zero(), zero(), zero()};
         // both outer loops stay rolled (9 copies of the z row instead of 27):
         // smaller code, fewer instruction-fetch stalls in the fused kernels
 #pragma unroll 1
         for (int ox = 0; ox < 3; ++ox) {
-            float B00[3] = {0.f, 0.f, 0.f}, B10[3] = {0.f, 0.f, 0.f}, B20[3] = {0.f, 0.f, 0.f};
-            float B01[3] = {0.f, 0.f, 0.f}, B02[3] = {0.f, 0.f, 0.f};
+            V3 B00 = zero(), B10 = zero(), B20 = zero(), B01 = zero(), B02 = zero();
             // the y loop stays rolled: fully unrolled, the 27 hoisted tile
             // loads and the partial sums exceed the register budget of the
             // high-occupancy launch configurations and spill
 #pragma unroll 1
             for (int oy = 0; oy < 3; ++oy) {
-                float A0[3] = {0.f, 0.f, 0.f}, A1[3] = {0.f, 0.f, 0.f}, A2[3] = {0.f, 0.f, 0.f};
+                V3 A0 = zero(), A1 = zero(), A2 = zero();
 #pragma unroll
                 for (int oz = 0; oz < 3; ++oz) {
                     const float4 g = fetch(ox, oy, oz);
-                    const float vi[3] = {g.x, g.y, g.z};
+                    const V3 vi{make_float2(g.x, g.y), g.z};
                     const float wz = st.w(2, oz), dz = st.dw(2, oz);
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        A0[c] = fmaf(wz, vi[c], A0[c]);
-                        if (oz > 0) A1[c] = fmaf((float)oz * wz, vi[c], A1[c]);
-                        A2[c] = fmaf(dz, vi[c], A2[c]);
-                    }
+                    A0 = fma3(wz, vi, A0);
+                    if (oz > 0) A1 = fma3((float)oz * wz, vi, A1);
+                    A2 = fma3(dz, vi, A2);
                 }
                 const float wy = st.w(1, oy), dy = st.dw(1, oy), wyo = (float)oy * wy;
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    B00[c] = fmaf(wy, A0[c], B00[c]);
-                    if (oy > 0) B10[c] = fmaf(wyo, A0[c], B10[c]);
-                    B20[c] = fmaf(dy, A0[c], B20[c]);
-                    B01[c] = fmaf(wy, A1[c], B01[c]);
-                    B02[c] = fmaf(wy, A2[c], B02[c]);
-                }
+                B00 = fma3(wy, A0, B00);
+                if (oy > 0) B10 = fma3(wyo, A0, B10);
+                B20 = fma3(dy, A0, B20);
+                B01 = fma3(wy, A1, B01);
+                B02 = fma3(wy, A2, B02);
             }
             const float wx = st.w(0, ox), dx = st.dw(0, ox), wxo = (float)ox * wx;
+            vs = fma3(wx, B00, vs);
+            if (ox > 0) Sv[0] = fma3(wxo, B00, Sv[0]);
+            Gv[0] = fma3(dx, B00, Gv[0]);
+            Sv[1] = fma3(wx, B10, Sv[1]);
+            Gv[1] = fma3(wx, B20, Gv[1]);
+            Sv[2] = fma3(wx, B01, Sv[2]);
+            Gv[2] = fma3(wx, B02, Gv[2]);
+        }
+        v[0] = vs.xy.x;
+        v[1] = vs.xy.y;
+        v[2] = vs.z;
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                v[c] = fmaf(wx, B00[c], v[c]);
-                if (ox > 0) S[c][0] = fmaf(wxo, B00[c], S[c][0]);
-                G[c][0] = fmaf(dx, B00[c], G[c][0]);
-                S[c][1] = fmaf(wx, B10[c], S[c][1]);
-                G[c][1] = fmaf(wx, B20[c], G[c][1]);
-                S[c][2] = fmaf(wx, B01[c], S[c][2]);
-                G[c][2] = fmaf(wx, B02[c], G[c][2]);
-            }
+        for (int b = 0; b < 3; ++b) {
+            S[0][b] = Sv[b].xy.x;
+            S[1][b] = Sv[b].xy.y;
+            S[2][b] = Sv[b].z;
+            G[0][b] = Gv[b].xy.x;
+            G[1][b] = Gv[b].xy.y;
+            G[2][b] = Gv[b].z;
         }
     } else {
 #pragma unroll
@@ -407,8 +422,23 @@ __device__ __forceinline__ void p2g_scatter(const Stencil<D>& st, const P2GSourc
         alpha[c] = a0;
     }
     if constexpr (D == 3) {
+        // The x and y components as one pair on the paired FP32 instructions
+        // of sm_100 (FFMA2 / FMUL2 / FADD2: two independent lanes per
+        // instruction, each rounded like its scalar form); z and the mass stay
+        // scalar.
+        float2 beta_xy[3], Ap_xy[3];
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            beta_xy[b] = make_float2(beta[0][b], beta[1][b]);
+            Ap_xy[b] = make_float2(Ap[0][b], Ap[1][b]);
+        }
+        const float2 alpha_xy = make_float2(alpha[0], alpha[1]);
         // x + k b for a stencil offset k = 0, 1, 2 without a multiply by 0 or 1
         auto off = [](float x, float b, int k) { return k == 0 ? x : (k == 1 ? x + b : fmaf(2.f, b, x)); };
+        auto off2 = [](float2 x, float2 b, int k) {
+            return k == 0 ? x : (k == 1 ? __fadd2_rn(x, b) : __ffma2_rn(make_float2(2.f, 2.f), b, x));
+        };
+        auto dup = [](float s) { return make_float2(s, s); };
 #pragma unroll
         for (int ox = 0; ox < 3; ++ox)
 #pragma unroll
@@ -416,21 +446,19 @@ __device__ __forceinline__ void p2g_scatter(const Stencil<D>& st, const P2GSourc
                 const float wx = st.w(0, ox), wy = st.w(1, oy);
                 const float P = wx * wy, Qx = st.dw(0, ox) * wy, Qy = wx * st.dw(1, oy);
                 const float Pm = P * src.m;
-                float U[3], V[3], W[3];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const float lin = off(off(alpha[c], beta[c][0], ox), beta[c][1], oy);
-                    U[c] = fmaf(P, lin, fmaf(Ap[c][1], Qy, Ap[c][0] * Qx));
-                    V[c] = P * beta[c][2];
-                    W[c] = P * Ap[c][2];
-                }
+                const float2 P2 = dup(P);
+                const float2 lin_xy = off2(off2(alpha_xy, beta_xy[0], ox), beta_xy[1], oy);
+                const float2 U_xy =
+                    __ffma2_rn(P2, lin_xy, __ffma2_rn(Ap_xy[1], dup(Qy), __fmul2_rn(Ap_xy[0], dup(Qx))));
+                const float2 V_xy = __fmul2_rn(P2, beta_xy[2]), W_xy = __fmul2_rn(P2, Ap_xy[2]);
+                const float lin_z = off(off(alpha[2], beta[2][0], ox), beta[2][1], oy);
+                const float U_z = fmaf(P, lin_z, fmaf(Ap[2][1], Qy, Ap[2][0] * Qx));
+                const float V_z = P * beta[2][2], W_z = P * Ap[2][2];
 #pragma unroll
                 for (int oz = 0; oz < 3; ++oz) {
                     const float wz = st.w(2, oz), dz = st.dw(2, oz);
-                    float out[3];
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) out[c] = fmaf(wz, off(U[c], V[c], oz), dz * W[c]);
-                    emit(ox, oy, oz, make_float4(out[0], out[1], out[2], Pm * wz));
+                    const float2 o_xy = __ffma2_rn(dup(wz), off2(U_xy, V_xy, oz), __fmul2_rn(dup(dz), W_xy));
+                    emit(ox, oy, oz, make_float4(o_xy.x, o_xy.y, fmaf(wz, off(U_z, V_z, oz), dz * W_z), Pm * wz));
                 }
             }
     } else {
