@@ -387,6 +387,9 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
         if ((rc = alloc((void**)&det_src, paged ? 16 : (size_t)src_planes * cap * sizeof(float), "source records")) !=
             MPM_OK)
             return rc;
+        if ((rc = alloc((void**)&det_sorted, paged ? 16 : (size_t)src_planes * cap * sizeof(float),
+                        "sorted source records")) != MPM_OK)
+            return rc;
     }
     if ((rc = alloc((void**)&seg_count, total_blocks * 4 * sizeof(int), "segment counts")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&seg_start, total_blocks * 4 * sizeof(int), "segment starts")) != MPM_OK) return rc;
@@ -683,7 +686,7 @@ void Engine::release() {
     }
     void* ptrs[] = {groups_d, scenes_d, grid_mom, grid_vel, err_d, keys[0], keys[1], vals[0], vals[1],
                     cell_count, seg_count, seg_start, sort_tmp, blk_flag, active, blk_epoch, counters, chunks,
-                    scan_tmp, pos_out, cell_end, det_src, sur_counts, speed_max, scene_time,
+                    scan_tmp, pos_out, cell_end, det_src, det_sorted, sur_counts, speed_max, scene_time,
                     pages.page, pages.slot_block, pages.free_slots};
     for (void* p : ptrs) cudaFree(p);
     pages = GridPages{};
@@ -694,7 +697,7 @@ void Engine::release() {
     keys[0] = keys[1] = nullptr;
     vals[0] = vals[1] = nullptr;
     cell_count = seg_count = seg_start = cell_end = nullptr;
-    det_src = nullptr;
+    det_src = det_sorted = nullptr;
     sort_tmp = nullptr;
     blk_flag = nullptr;
     active = blk_epoch = counters = nullptr;
@@ -969,12 +972,19 @@ void Engine::enqueue_det_p2g() {
         note_launch("cub::DeviceRadixSort::SortPairs");
         k_det_ranges<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys[1], n_particles, cell_count, cell_end);
         note_launch("k_det_ranges");
+        if (dim == 3)
+            k_det_permute<3><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(det_src, det_sorted, cap, vals[1],
+                                                                                n_particles);
+        else
+            k_det_permute<2><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(det_src, det_sorted, cap, vals[1],
+                                                                                n_particles);
+        note_launch("k_det_permute");
     }
     if (dim == 3)
-        k_det_gather<3><<<update_ctas, 256, 0, stream>>>(det_src, cap, vals[1], cell_count, cell_end, active,
+        k_det_gather<3><<<update_ctas, 256, 0, stream>>>(det_sorted, cap, cell_count, cell_end, active,
                                                          counters + CNT_ACTIVE, scenes_d, n_scenes, grid_mom);
     else
-        k_det_gather<2><<<update_ctas, 256, 0, stream>>>(det_src, cap, vals[1], cell_count, cell_end, active,
+        k_det_gather<2><<<update_ctas, 256, 0, stream>>>(det_sorted, cap, cell_count, cell_end, active,
                                                          counters + CNT_ACTIVE, scenes_d, n_scenes, grid_mom);
     note_launch("k_det_gather");
     if (n_particles > 0) {

@@ -7,6 +7,8 @@
 // node; a stable radix sort groups the records by base node; then each grid
 // node sums, in a fixed order (stencil offset, then sorted position), the
 // records of the 27 base nodes whose stencils cover it, and stores the sum.
+// The records are copied into sorted order once (k_det_permute), so the sum
+// reads each base node's records as one contiguous run.
 // Particles stay in creation order in this mode and the grid update visits the
 // blocks the stencils touched, as in the binned path.
 #pragma once
@@ -95,11 +97,23 @@ __global__ void __launch_bounds__(256) k_det_reset(const unsigned long long* __r
     cell_end[k] = 0;
 }
 
+// The records in sorted order: slot j of `dst` gets the record of particle
+// order[j] (the out-of-grid particles, sorted last, copy records nobody reads)
+template <int D>
+__global__ void __launch_bounds__(256) k_det_permute(const float* __restrict__ src, float* __restrict__ dst,
+                                                     long long cap, const unsigned* __restrict__ order, long long n) {
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const long long p = order[j];
+#pragma unroll
+    for (int k = 0; k < SrcPlanes<D>::COUNT; ++k) dst[k * cap + j] = src[k * cap + p];
+}
+
 // Every node of the active blocks sums the records of the base nodes
-// node - o, o in {0,1,2}^D, in the order (o, sorted position), and stores it.
+// node - o, o in {0,1,2}^D, in the order (o, sorted position), and stores it
+// (src: the records in sorted order).
 template <int D>
 __global__ void __launch_bounds__(256) k_det_gather(const float* __restrict__ src, long long cap,
-                                                    const unsigned* __restrict__ order,
                                                     const int* __restrict__ cell_start,
                                                     const int* __restrict__ cell_end, const int* __restrict__ active,
                                                     const int* __restrict__ n_active,
@@ -127,20 +141,19 @@ __global__ void __launch_bounds__(256) k_det_gather(const float* __restrict__ sr
                     const int j1 = cell_end[cell];
                     const int o[3] = {ox, oy, oz};
                     for (int j = cell_start[cell]; j < j1; ++j) {
-                        const long long p = order[j];
                         Stencil<D> st;
                         P2GSource<D> s;
 #pragma unroll
                         for (int a = 0; a < D; ++a) {
-                            st.fx[a] = src[(SP::FX + a) * cap + p];
-                            s.mv[a] = src[(SP::MV + a) * cap + p];
+                            st.fx[a] = src[(SP::FX + a) * cap + j];
+                            s.mv[a] = src[(SP::MV + a) * cap + j];
                         }
 #pragma unroll
                         for (int k = 0; k < D * D; ++k) {
-                            s.mC[k] = src[(SP::MC + k) * cap + p];
-                            s.A[k] = src[(SP::A + k) * cap + p];
+                            s.mC[k] = src[(SP::MC + k) * cap + j];
+                            s.A[k] = src[(SP::A + k) * cap + j];
                         }
-                        s.m = src[SP::M * cap + p];
+                        s.m = src[SP::M * cap + j];
                         const float4 c = p2g_node<D>(st, s, o, sc.h, sc.inv_h);
                         acc[0] += c.x;
                         acc[1] += c.y;
