@@ -4,6 +4,8 @@
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+#include <cub/iterator/counting_input_iterator.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -35,6 +37,7 @@ enum {
     CNT_REBINS = 9,
     CNT_UPDATE_DONE = 10,
     CNT_POOL_FREE = 11,  // paged grid: height of the free stack
+    CNT_DET_BLOCKS = 12, // deterministic P2G: length of the ascending list of marked blocks
     CNT_N = 16
 };
 
@@ -387,8 +390,11 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
         if ((rc = alloc((void**)&det_src, paged ? 16 : (size_t)src_planes * cap * sizeof(float), "source records")) !=
             MPM_OK)
             return rc;
-        if ((rc = alloc((void**)&det_sorted, paged ? 16 : (size_t)src_planes * cap * sizeof(float),
+        const int src_stride = dim == 3 ? SrcPlanes<3>::STRIDE : SrcPlanes<2>::STRIDE;
+        if ((rc = alloc((void**)&det_sorted, paged ? 16 : (size_t)src_stride * cap * sizeof(float),
                         "sorted source records")) != MPM_OK)
+            return rc;
+        if ((rc = alloc((void**)&det_blocks, paged ? 16 : total_blocks * sizeof(int), "sorted block list")) != MPM_OK)
             return rc;
     }
     if ((rc = alloc((void**)&seg_count, total_blocks * 4 * sizeof(int), "segment counts")) != MPM_OK) return rc;
@@ -406,6 +412,13 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     det_key_bits = 1;
     while (det_key_bits < 64 && (1LL << det_key_bits) <= total_blocks * 64) ++det_key_bits;
     cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp_bytes, keys[0], keys[1], vals[0], vals[1], (int)cap, 0, 64);
+    {
+        // the deterministic path's ascending list of marked blocks shares the temp space
+        size_t sel = 0;
+        cub::DeviceSelect::Flagged(nullptr, sel, cub::CountingInputIterator<int>(0), blk_flag, det_blocks,
+                                   counters + CNT_DET_BLOCKS, (int)total_blocks);
+        sort_tmp_bytes = std::max(sort_tmp_bytes, sel);
+    }
     if ((rc = alloc(&sort_tmp, sort_tmp_bytes, "sort temp")) != MPM_OK) return rc;
     cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp_bytes, seg_count, seg_start, (int)(total_blocks * 4));
     if ((rc = alloc(&scan_tmp, scan_tmp_bytes, "scan temp")) != MPM_OK) return rc;
@@ -686,7 +699,7 @@ void Engine::release() {
     }
     void* ptrs[] = {groups_d, scenes_d, grid_mom, grid_vel, err_d, keys[0], keys[1], vals[0], vals[1],
                     cell_count, seg_count, seg_start, sort_tmp, blk_flag, active, blk_epoch, counters, chunks,
-                    scan_tmp, pos_out, cell_end, det_src, det_sorted, sur_counts, speed_max, scene_time,
+                    scan_tmp, pos_out, cell_end, det_src, det_sorted, det_blocks, sur_counts, speed_max, scene_time,
                     pages.page, pages.slot_block, pages.free_slots};
     for (void* p : ptrs) cudaFree(p);
     pages = GridPages{};
@@ -698,6 +711,7 @@ void Engine::release() {
     vals[0] = vals[1] = nullptr;
     cell_count = seg_count = seg_start = cell_end = nullptr;
     det_src = det_sorted = nullptr;
+    det_blocks = nullptr;
     sort_tmp = nullptr;
     blk_flag = nullptr;
     active = blk_epoch = counters = nullptr;
@@ -973,19 +987,24 @@ void Engine::enqueue_det_p2g() {
         k_det_ranges<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys[1], n_particles, cell_count, cell_end);
         note_launch("k_det_ranges");
         if (dim == 3)
-            k_det_permute<3><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(det_src, det_sorted, cap, vals[1],
-                                                                                n_particles);
+            k_det_permute<3><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(det_src, (float4*)det_sorted, cap,
+                                                                                vals[1], n_particles);
         else
-            k_det_permute<2><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(det_src, det_sorted, cap, vals[1],
-                                                                                n_particles);
+            k_det_permute<2><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(det_src, (float4*)det_sorted, cap,
+                                                                                vals[1], n_particles);
         note_launch("k_det_permute");
     }
+    // the blocks the source records marked, in ascending order: neighbouring
+    // blocks then sum at about the same time and share the records in L2
+    cub::DeviceSelect::Flagged(sort_tmp, sort_tmp_bytes, cub::CountingInputIterator<int>(0), blk_flag, det_blocks,
+                               counters + CNT_DET_BLOCKS, (int)total_blocks, stream);
+    note_launch("cub::DeviceSelect::Flagged");
     if (dim == 3)
-        k_det_gather<3><<<update_ctas, 256, 0, stream>>>(det_sorted, cap, cell_count, cell_end, active,
-                                                         counters + CNT_ACTIVE, scenes_d, n_scenes, grid_mom);
+        k_det_gather<3><<<update_ctas, 256, 0, stream>>>((const float4*)det_sorted, cell_count, cell_end, det_blocks,
+                                                         counters + CNT_DET_BLOCKS, scenes_d, n_scenes, grid_mom);
     else
-        k_det_gather<2><<<update_ctas, 256, 0, stream>>>(det_sorted, cap, cell_count, cell_end, active,
-                                                         counters + CNT_ACTIVE, scenes_d, n_scenes, grid_mom);
+        k_det_gather<2><<<update_ctas, 256, 0, stream>>>((const float4*)det_sorted, cell_count, cell_end, det_blocks,
+                                                         counters + CNT_DET_BLOCKS, scenes_d, n_scenes, grid_mom);
     note_launch("k_det_gather");
     if (n_particles > 0) {
         k_det_reset<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys[1], n_particles, cell_count, cell_end);

@@ -58,6 +58,7 @@ struct Engine {
     int* cell_end = nullptr;    // deterministic mode: end of each base node's records
     float* det_src = nullptr;   // deterministic mode: P2G source records
     float* det_sorted = nullptr;  // the same records in sorted order
+    int* det_blocks = nullptr;    // the blocks they mark, ascending
     int det_key_bits = 64;
     bool sorted_order = false;  // particles permuted away from creation order
     int* seg_count = nullptr;   // per (block, material)

@@ -7,8 +7,9 @@
 // node; a stable radix sort groups the records by base node; then each grid
 // node sums, in a fixed order (stencil offset, then sorted position), the
 // records of the 27 base nodes whose stencils cover it, and stores the sum.
-// The records are copied into sorted order once (k_det_permute), so the sum
-// reads each base node's records as one contiguous run.
+// The records are copied into sorted order once (k_det_permute), each record
+// contiguous, so the sum reads each base node's records as one contiguous run
+// of whole records (a few float4 loads each).
 // Particles stay in creation order in this mode and the grid update visits the
 // blocks the stencils touched, as in the binned path.
 #pragma once
@@ -25,6 +26,8 @@ template <int D>
 struct SrcPlanes {
     static constexpr int FX = 0, MV = D, MC = 2 * D, A = 2 * D + D * D, M = 2 * D + 2 * D * D;
     static constexpr int COUNT = 2 * D + 2 * D * D + 1;
+    // a record of the sorted copy: COUNT floats padded to whole float4s
+    static constexpr int STRIDE = (COUNT + 3) / 4 * 4;
 };
 
 constexpr unsigned long long kNoCell = ~0ull;
@@ -97,23 +100,29 @@ __global__ void __launch_bounds__(256) k_det_reset(const unsigned long long* __r
     cell_end[k] = 0;
 }
 
-// The records in sorted order: slot j of `dst` gets the record of particle
-// order[j] (the out-of-grid particles, sorted last, copy records nobody reads)
+// The records in sorted order: record j of `dst` (STRIDE floats, planes in
+// the same order) gets the record of particle order[j] (the out-of-grid
+// particles, sorted last, copy records nobody reads)
 template <int D>
-__global__ void __launch_bounds__(256) k_det_permute(const float* __restrict__ src, float* __restrict__ dst,
+__global__ void __launch_bounds__(256) k_det_permute(const float* __restrict__ src, float4* __restrict__ dst,
                                                      long long cap, const unsigned* __restrict__ order, long long n) {
+    using SP = SrcPlanes<D>;
     const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const long long p = order[j];
+    float r[SP::STRIDE];
 #pragma unroll
-    for (int k = 0; k < SrcPlanes<D>::COUNT; ++k) dst[k * cap + j] = src[k * cap + p];
+    for (int k = 0; k < SP::STRIDE; ++k) r[k] = k < SP::COUNT ? src[k * cap + p] : 0.f;
+#pragma unroll
+    for (int q = 0; q < SP::STRIDE / 4; ++q)
+        dst[j * (SP::STRIDE / 4) + q] = make_float4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
 }
 
 // Every node of the active blocks sums the records of the base nodes
 // node - o, o in {0,1,2}^D, in the order (o, sorted position), and stores it
-// (src: the records in sorted order).
+// (src: the records in sorted order, k_det_permute's layout).
 template <int D>
-__global__ void __launch_bounds__(256) k_det_gather(const float* __restrict__ src, long long cap,
+__global__ void __launch_bounds__(256) k_det_gather(const float4* __restrict__ src,
                                                     const int* __restrict__ cell_start,
                                                     const int* __restrict__ cell_end, const int* __restrict__ active,
                                                     const int* __restrict__ n_active,
@@ -141,19 +150,28 @@ __global__ void __launch_bounds__(256) k_det_gather(const float* __restrict__ sr
                     const int j1 = cell_end[cell];
                     const int o[3] = {ox, oy, oz};
                     for (int j = cell_start[cell]; j < j1; ++j) {
+                        float r[SP::STRIDE];
+#pragma unroll
+                        for (int q = 0; q < SP::STRIDE / 4; ++q) {
+                            const float4 v = src[(long long)j * (SP::STRIDE / 4) + q];
+                            r[4 * q] = v.x;
+                            r[4 * q + 1] = v.y;
+                            r[4 * q + 2] = v.z;
+                            r[4 * q + 3] = v.w;
+                        }
                         Stencil<D> st;
                         P2GSource<D> s;
 #pragma unroll
                         for (int a = 0; a < D; ++a) {
-                            st.fx[a] = src[(SP::FX + a) * cap + j];
-                            s.mv[a] = src[(SP::MV + a) * cap + j];
+                            st.fx[a] = r[SP::FX + a];
+                            s.mv[a] = r[SP::MV + a];
                         }
 #pragma unroll
                         for (int k = 0; k < D * D; ++k) {
-                            s.mC[k] = src[(SP::MC + k) * cap + j];
-                            s.A[k] = src[(SP::A + k) * cap + j];
+                            s.mC[k] = r[SP::MC + k];
+                            s.A[k] = r[SP::A + k];
                         }
-                        s.m = src[SP::M * cap + j];
+                        s.m = r[SP::M];
                         const float4 c = p2g_node<D>(st, s, o, sc.h, sc.inv_h);
                         acc[0] += c.x;
                         acc[1] += c.y;
