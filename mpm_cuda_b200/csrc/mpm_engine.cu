@@ -38,6 +38,7 @@ enum {
     CNT_UPDATE_DONE = 10,
     CNT_POOL_FREE = 11,  // paged grid: height of the free stack
     CNT_DET_BLOCKS = 12, // deterministic P2G: length of the ascending list of marked blocks
+    CNT_DET_RUNS = 13,   // deterministic P2G: number of runs of records sharing a base node
     CNT_N = 16
 };
 
@@ -396,6 +397,10 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
             return rc;
         if ((rc = alloc((void**)&det_blocks, paged ? 16 : total_blocks * sizeof(int), "sorted block list")) != MPM_OK)
             return rc;
+        if (deterministic() && (rc = alloc_det_partials()) != MPM_OK) {
+            msg = "mpm_create: " + last_error;
+            return rc;
+        }
     }
     if ((rc = alloc((void**)&seg_count, total_blocks * 4 * sizeof(int), "segment counts")) != MPM_OK) return rc;
     if ((rc = alloc((void**)&seg_start, total_blocks * 4 * sizeof(int), "segment starts")) != MPM_OK) return rc;
@@ -417,6 +422,10 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
         size_t sel = 0;
         cub::DeviceSelect::Flagged(nullptr, sel, cub::CountingInputIterator<int>(0), blk_flag, det_blocks,
                                    counters + CNT_DET_BLOCKS, (int)total_blocks);
+        sort_tmp_bytes = std::max(sort_tmp_bytes, sel);
+        // and the list of runs of sorted records
+        cub::DeviceSelect::If(nullptr, sel, cub::CountingInputIterator<int>(0), det_runs, counters + CNT_DET_RUNS,
+                              (int)cap, RunStart{keys[1]});
         sort_tmp_bytes = std::max(sort_tmp_bytes, sel);
     }
     if ((rc = alloc(&sort_tmp, sort_tmp_bytes, "sort temp")) != MPM_OK) return rc;
@@ -699,7 +708,8 @@ void Engine::release() {
     }
     void* ptrs[] = {groups_d, scenes_d, grid_mom, grid_vel, err_d, keys[0], keys[1], vals[0], vals[1],
                     cell_count, seg_count, seg_start, sort_tmp, blk_flag, active, blk_epoch, counters, chunks,
-                    scan_tmp, pos_out, cell_end, det_src, det_sorted, det_blocks, sur_counts, speed_max, scene_time,
+                    scan_tmp, pos_out, cell_end, det_src, det_sorted, det_blocks, det_runs, det_partial,
+                    sur_counts, speed_max, scene_time,
                     pages.page, pages.slot_block, pages.free_slots};
     for (void* p : ptrs) cudaFree(p);
     pages = GridPages{};
@@ -711,7 +721,8 @@ void Engine::release() {
     vals[0] = vals[1] = nullptr;
     cell_count = seg_count = seg_start = cell_end = nullptr;
     det_src = det_sorted = nullptr;
-    det_blocks = nullptr;
+    det_blocks = det_runs = nullptr;
+    det_partial = nullptr;
     sort_tmp = nullptr;
     blk_flag = nullptr;
     active = blk_epoch = counters = nullptr;
@@ -994,18 +1005,32 @@ void Engine::enqueue_det_p2g() {
                                                                                 vals[1], n_particles);
         note_launch("k_det_permute");
     }
-    // the blocks the source records marked, in ascending order: neighbouring
-    // blocks then sum at about the same time and share the records in L2
+    if (n_particles > 0) {
+        // the runs of records sharing a base node, and their partial sums
+        cub::DeviceSelect::If(sort_tmp, sort_tmp_bytes, cub::CountingInputIterator<int>(0), det_runs,
+                              counters + CNT_DET_RUNS, (int)n_particles, RunStart{keys[1]}, stream);
+        note_launch("cub::DeviceSelect::If");
+        if (dim == 3)
+            k_det_partials<3><<<num_sms * 8, 64, 0, stream>>>((const float4*)det_sorted, keys[1], det_runs,
+                                                              counters + CNT_DET_RUNS, cell_end, scenes_d, n_scenes,
+                                                              det_partial);
+        else
+            k_det_partials<2><<<num_sms * 8, 64, 0, stream>>>((const float4*)det_sorted, keys[1], det_runs,
+                                                              counters + CNT_DET_RUNS, cell_end, scenes_d, n_scenes,
+                                                              det_partial);
+        note_launch("k_det_partials");
+    }
+    // the blocks the source records marked, in ascending order
     cub::DeviceSelect::Flagged(sort_tmp, sort_tmp_bytes, cub::CountingInputIterator<int>(0), blk_flag, det_blocks,
                                counters + CNT_DET_BLOCKS, (int)total_blocks, stream);
     note_launch("cub::DeviceSelect::Flagged");
     if (dim == 3)
-        k_det_gather<3><<<update_ctas, 256, 0, stream>>>((const float4*)det_sorted, cell_count, cell_end, det_blocks,
-                                                         counters + CNT_DET_BLOCKS, scenes_d, n_scenes, grid_mom);
+        k_det_sum<3><<<update_ctas, 256, 0, stream>>>(det_partial, cell_count, cell_end, det_blocks,
+                                                      counters + CNT_DET_BLOCKS, scenes_d, n_scenes, grid_mom);
     else
-        k_det_gather<2><<<update_ctas, 256, 0, stream>>>((const float4*)det_sorted, cell_count, cell_end, det_blocks,
-                                                         counters + CNT_DET_BLOCKS, scenes_d, n_scenes, grid_mom);
-    note_launch("k_det_gather");
+        k_det_sum<2><<<update_ctas, 256, 0, stream>>>(det_partial, cell_count, cell_end, det_blocks,
+                                                      counters + CNT_DET_BLOCKS, scenes_d, n_scenes, grid_mom);
+    note_launch("k_det_sum");
     if (n_particles > 0) {
         k_det_reset<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys[1], n_particles, cell_count, cell_end);
         note_launch("k_det_reset");
@@ -1535,6 +1560,22 @@ int Engine::bin_stats(int64_t* fallbacks, int64_t* rebins) {
     return MPM_OK;
 }
 
+// The deterministic path's partial sums (3^D float4 per particle slot) and run
+// list, allocated when the path is first chosen
+int Engine::alloc_det_partials() {
+    if (det_partial) return MPM_OK;
+    const int k = dim == 3 ? 27 : 9;
+    if (cudaMalloc((void**)&det_partial, (size_t)cap * k * sizeof(float4)) != cudaSuccess ||
+        cudaMalloc((void**)&det_runs, (size_t)cap * sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(det_partial);
+        det_partial = nullptr;
+        last_error = "mpm: out of device memory for the deterministic path's partial sums";
+        return MPM_ERR_NOMEM;
+    }
+    return MPM_OK;
+}
+
 int Engine::set_p2g_mode(int mode) {
     if (paged && mode != MPM_P2G_ATOMIC) {
         last_error = "mpm_set_p2g_mode: a paged grid runs in MPM_P2G_ATOMIC only";
@@ -1554,6 +1595,10 @@ int Engine::set_p2g_mode(int mode) {
         if (rc != MPM_OK) return rc;
     }
     MPM_CUDA_TRY(cudaStreamSynchronize(stream), "stream sync");
+    if (mode == MPM_P2G_DETERMINISTIC) {
+        const int rc = alloc_det_partials();
+        if (rc != MPM_OK) return rc;
+    }
     opt.p2g_mode = mode;
     drop_graphs();
     grid_dirty = true;

@@ -59,6 +59,8 @@ struct Engine {
     float* det_src = nullptr;   // deterministic mode: P2G source records
     float* det_sorted = nullptr;  // the same records in sorted order
     int* det_blocks = nullptr;    // the blocks they mark, ascending
+    int* det_runs = nullptr;      // first sorted position of each run sharing a base node
+    float4* det_partial = nullptr;  // per (run, stencil offset) partial sums (allocated on first use)
     int det_key_bits = 64;
     bool sorted_order = false;  // particles permuted away from creation order
     int* seg_count = nullptr;   // per (block, material)
@@ -149,6 +151,7 @@ struct Engine {
     int get_grid(int scene, float* mass, float* vel);
     int count_active_nodes(int scene, int64_t* n);
     int set_p2g_mode(int mode);
+    int alloc_det_partials();
     int set_stress_mode(int mode, Surrogate* s);
     int stress_stats(int64_t* net, int64_t* fallback);
     int scene_time_of(int scene, double* t, float* dt);

@@ -180,44 +180,6 @@ __device__ __forceinline__ void source_from_tau(const float* v, const float* C, 
     src.m = g.p_mass;
 }
 
-// contribution of the source to stencil node `o` (offsets 0..2 per axis)
-template <int D>
-__device__ __forceinline__ float4 p2g_node(const Stencil<D>& st, const P2GSource<D>& src,
-                                           const int* o, float h, float inv_h) {
-    float wa[3], dwa[3];
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-        wa[a] = st.w(a, o[a]);
-        dwa[a] = st.dw(a, o[a]);
-    }
-    float w = wa[0] * wa[1];
-    float gw[D];
-    if constexpr (D == 3) {
-        w *= wa[2];
-        gw[0] = inv_h * dwa[0] * wa[1] * wa[2];
-        gw[1] = inv_h * wa[0] * dwa[1] * wa[2];
-        gw[2] = inv_h * wa[0] * wa[1] * dwa[2];
-    } else {
-        gw[0] = inv_h * dwa[0] * wa[1];
-        gw[1] = inv_h * wa[0] * dwa[1];
-    }
-    float dx[D];
-#pragma unroll
-    for (int a = 0; a < D; ++a) dx[a] = ((float)o[a] - st.fx[a]) * h;
-    float out[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-        float cdx = src.mv[a];
-#pragma unroll
-        for (int b = 0; b < D; ++b) cdx = fmaf(src.mC[a * D + b], dx[b], cdx);
-        float f = 0.f;
-#pragma unroll
-        for (int b = 0; b < D; ++b) f = fmaf(src.A[a * D + b], gw[b], f);
-        out[a] = fmaf(w, cdx, f);
-    }
-    return make_float4(out[0], out[1], out[2], w * src.m);
-}
-
 // G2P accumulators (InterpolateAndMove, MPMCUDA.cu:500-587)
 template <int D>
 struct G2PAcc {
