@@ -56,8 +56,11 @@ enum mpm_p2g_mode {
                                   grid velocities and scatters with FP32
                                   vector reductions to global memory (fast;
                                   summation order varies run to run) */
-    MPM_P2G_DETERMINISTIC = 1, /* cell-sorted gather reduction: bitwise
-                                  identical results across runs */
+    MPM_P2G_DETERMINISTIC = 1, /* records sorted by base node, summed in a
+                                  fixed order (per-run partial sums, then
+                                  per-node sums): bitwise identical results
+                                  across runs; 27 float4 of partial sums per
+                                  particle slot, allocated when first chosen */
     MPM_P2G_DIRECT = 2         /* unbinned: one thread per particle, stencil
                                   straight to global memory (the reference's
                                   kernel structure; for comparison) */
@@ -309,7 +312,8 @@ int mpm_last_error(mpm_handle *h, char *buf, size_t cap);
  *   MPM_P2G_ATOMIC:  rebin (time of one re-binning; they run every
  *                    rebin_interval substeps as in mpm_step), grid_update, g2p2g
  *   MPM_P2G_DIRECT:  p2g, grid_update, g2p
- *   MPM_P2G_DETERMINISTIC: grid_update, g2p, p2g (source + sort + gather)
+ *   MPM_P2G_DETERMINISTIC: grid_update, g2p, p2g (source records, sort,
+ *                    partial sums, node sums)
  * *n_written receives the number of stages written. */
 int mpm_profile_stages(mpm_handle *h, int n_substeps, float *out_ms, int n_out,
                        int *n_written);

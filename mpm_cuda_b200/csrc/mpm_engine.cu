@@ -414,6 +414,8 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
     // partial chunk per non-empty block
     list_cap = cap / kMinChunkParticles + std::min<long long>(cap, total_blocks) + 1;
     if ((rc = alloc((void**)&chunks, kMats * list_cap * sizeof(Chunk), "chunks")) != MPM_OK) return rc;
+    // bits of the deterministic path's sort keys: node indices and the
+    // no-cell key (the node count) are all below 2^det_key_bits
     det_key_bits = 1;
     while (det_key_bits < 64 && (1LL << det_key_bits) <= total_blocks * 64) ++det_key_bits;
     cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp_bytes, keys[0], keys[1], vals[0], vals[1], (int)cap, 0, 64);
@@ -425,7 +427,7 @@ int Engine::create(const mpm_scene_desc* scenes, int n_scenes, const mpm_options
         sort_tmp_bytes = std::max(sort_tmp_bytes, sel);
         // and the list of runs of sorted records
         cub::DeviceSelect::If(nullptr, sel, cub::CountingInputIterator<int>(0), det_runs, counters + CNT_DET_RUNS,
-                              (int)cap, RunStart{keys[1]});
+                              (int)cap, RunStart{keys[1], det_no_cell()});
         sort_tmp_bytes = std::max(sort_tmp_bytes, sel);
     }
     if ((rc = alloc(&sort_tmp, sort_tmp_bytes, "sort temp")) != MPM_OK) return rc;
@@ -984,18 +986,20 @@ void Engine::enqueue_det_p2g() {
     if (n_particles > 0) {
         if (dim == 3)
             k_det_source<3><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(
-                buf(cur), n_particles, groups_d, scenes_d, det_src, cap, keys[0], vals[0], blk_flag, active,
-                counters + CNT_ACTIVE, err_d);
+                buf(cur), n_particles, groups_d, scenes_d, det_src, cap, keys[0], det_no_cell(), vals[0], blk_flag,
+                active, counters + CNT_ACTIVE, err_d);
         else
             k_det_source<2><<<grid_blocks(n_particles, 128), 128, 0, stream>>>(
-                buf(cur), n_particles, groups_d, scenes_d, det_src, cap, keys[0], vals[0], blk_flag, active,
-                counters + CNT_ACTIVE, err_d);
+                buf(cur), n_particles, groups_d, scenes_d, det_src, cap, keys[0], det_no_cell(), vals[0], blk_flag,
+                active, counters + CNT_ACTIVE, err_d);
         note_launch("k_det_source");
-        // the no-cell key is all ones: sort on every bit so it lands last
+        // keys are node indices below the no-cell key (the node count), which
+        // sorts last: the sort needs only the bits that hold the node count
         cub::DeviceRadixSort::SortPairs(sort_tmp, sort_tmp_bytes, keys[0], keys[1], vals[0], vals[1],
-                                        (int)n_particles, 0, 64, stream);
+                                        (int)n_particles, 0, det_key_bits, stream);
         note_launch("cub::DeviceRadixSort::SortPairs");
-        k_det_ranges<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys[1], n_particles, cell_count, cell_end);
+        k_det_ranges<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys[1], n_particles, det_no_cell(),
+                                                                        cell_count, cell_end);
         note_launch("k_det_ranges");
         if (dim == 3)
             k_det_permute<3><<<grid_blocks(n_particles, 256), 256, 0, stream>>>(det_src, (float4*)det_sorted, cap,
@@ -1008,7 +1012,7 @@ void Engine::enqueue_det_p2g() {
     if (n_particles > 0) {
         // the runs of records sharing a base node, and their partial sums
         cub::DeviceSelect::If(sort_tmp, sort_tmp_bytes, cub::CountingInputIterator<int>(0), det_runs,
-                              counters + CNT_DET_RUNS, (int)n_particles, RunStart{keys[1]}, stream);
+                              counters + CNT_DET_RUNS, (int)n_particles, RunStart{keys[1], det_no_cell()}, stream);
         note_launch("cub::DeviceSelect::If");
         if (dim == 3)
             k_det_partials<3><<<num_sms * 8, 64, 0, stream>>>((const float4*)det_sorted, keys[1], det_runs,
@@ -1032,7 +1036,8 @@ void Engine::enqueue_det_p2g() {
                                                       counters + CNT_DET_BLOCKS, scenes_d, n_scenes, grid_mom);
     note_launch("k_det_sum");
     if (n_particles > 0) {
-        k_det_reset<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys[1], n_particles, cell_count, cell_end);
+        k_det_reset<<<grid_blocks(n_particles, 256), 256, 0, stream>>>(keys[1], n_particles, det_no_cell(),
+                                                                       cell_count, cell_end);
         note_launch("k_det_reset");
     }
 }

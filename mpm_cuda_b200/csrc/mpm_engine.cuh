@@ -62,6 +62,8 @@ struct Engine {
     int* det_runs = nullptr;      // first sorted position of each run sharing a base node
     float4* det_partial = nullptr;  // per (run, stencil offset) partial sums (allocated on first use)
     int det_key_bits = 64;
+    // sort key of a particle whose stencil left the grid: one past the last node
+    unsigned long long det_no_cell() const { return (unsigned long long)total_blocks * 64; }
     bool sorted_order = false;  // particles permuted away from creation order
     int* seg_count = nullptr;   // per (block, material)
     int* seg_start = nullptr;

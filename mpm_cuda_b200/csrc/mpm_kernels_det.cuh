@@ -32,12 +32,12 @@ struct SrcPlanes {
     static constexpr int STRIDE = (COUNT + 3) / 4 * 4;
 };
 
-constexpr unsigned long long kNoCell = ~0ull;
 
 template <int D>
 __global__ void __launch_bounds__(128) k_det_source(ParticleBuf pb, long long n, const GroupParams* __restrict__ groups,
                                                     const SceneParams* __restrict__ scenes, float* __restrict__ src,
                                                     long long cap, unsigned long long* __restrict__ keys,
+                                                    unsigned long long no_cell,
                                                     unsigned* __restrict__ vals, unsigned* __restrict__ blk_flag,
                                                     int* __restrict__ active, int* __restrict__ n_active,
                                                     unsigned* err_word) {
@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(128) k_det_source(ParticleBuf pb, long long n,
     unsigned err = 0;
     Stencil<D> st;
     if (!make_stencil<D>(x, sc, st, err)) {
-        keys[i] = kNoCell;
+        keys[i] = no_cell;
         atomicOr(err_word, err);
         return;
     }
@@ -83,21 +83,23 @@ __global__ void __launch_bounds__(128) k_det_source(ParticleBuf pb, long long n,
 
 // [cell_start, cell_end) of every base node in the sorted records
 __global__ void __launch_bounds__(256) k_det_ranges(const unsigned long long* __restrict__ keys, long long n,
-                                                    int* __restrict__ cell_start, int* __restrict__ cell_end) {
+                                                    unsigned long long no_cell, int* __restrict__ cell_start,
+                                                    int* __restrict__ cell_end) {
     const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const unsigned long long k = keys[j];
-    if (k == kNoCell) return;
+    if (k == no_cell) return;
     if (j == 0 || keys[j - 1] != k) cell_start[k] = (int)j;
     if (j == n - 1 || keys[j + 1] != k) cell_end[k] = (int)j + 1;
 }
 
 __global__ void __launch_bounds__(256) k_det_reset(const unsigned long long* __restrict__ keys, long long n,
-                                                   int* __restrict__ cell_start, int* __restrict__ cell_end) {
+                                                   unsigned long long no_cell, int* __restrict__ cell_start,
+                                                   int* __restrict__ cell_end) {
     const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const unsigned long long k = keys[j];
-    if (k == kNoCell) return;
+    if (k == no_cell) return;
     cell_start[k] = 0;
     cell_end[k] = 0;
 }
@@ -123,8 +125,9 @@ __global__ void __launch_bounds__(256) k_det_permute(const float* __restrict__ s
 // Run starts in the sorted keys (the out-of-grid particles, sorted last, start none)
 struct RunStart {
     const unsigned long long* keys;
+    unsigned long long no_cell;
     __device__ __forceinline__ bool operator()(int j) const {
-        return keys[j] != kNoCell && (j == 0 || keys[j - 1] != keys[j]);
+        return keys[j] != no_cell && (j == 0 || keys[j - 1] != keys[j]);
     }
 };
 
