@@ -430,6 +430,34 @@ def test_deterministic_mode_is_bitwise_reproducible(gpu):
     assert np.array_equal(g0[0], g1[0]) and np.array_equal(g0[1], g1[1])
 
 
+@pytest.mark.parametrize("d", [2, 3])
+def test_deterministic_out_of_grid_particle_is_left_out_exactly(gpu, d):
+    # a particle whose stencil leaves the grid gets the sort key past the last
+    # node: it sorts after every run, starts none, and adds nothing, so the
+    # other particles and the grid come out bitwise equal to a run without it
+    sc = blob_scene(d, "jello", seed=71)
+    g = sc.groups[0]
+    extra = blob_scene(d, "jello", seed=71)
+    eg = extra.groups[0]
+    out = np.float32([0.999] + [0.5] * (d - 1))
+    for k in ("x", "v", "C", "F", "aux"):
+        a = getattr(eg, k)
+        setattr(eg, k, np.concatenate([a, a[:1]], axis=0))
+    eg.x[-1] = out
+    with Simulation([sc], p2g_mode=L.P2G_DETERMINISTIC) as ref, \
+            Simulation([extra], p2g_mode=L.P2G_DETERMINISTIC) as sim:
+        ref.step(3)
+        want, want_grid = ref.get_state(0), ref.get_grid(0)
+        assert sim.step_status(3) == L.ERR_SIM
+        assert sim.device_errors() & L.DEVERR_OUT_OF_GRID
+        got, got_grid = sim.get_state(0), sim.get_grid(0)
+    n = g.n
+    for k in ("x", "v", "C", "F", "aux"):
+        assert np.array_equal(got[k][:n], want[k]), k
+    assert np.array_equal(got["x"][n], out)  # left where it was
+    assert np.array_equal(got_grid[0], want_grid[0]) and np.array_equal(got_grid[1], want_grid[1])
+
+
 def test_deterministic_after_binned_steps_is_reproducible(gpu):
     # binned steps permute the particles (atomically ranked sort keys); the
     # deterministic mode first restores creation order, so two handles whose
