@@ -4,7 +4,8 @@
 // FP32 atomics make the order of a node's additions depend on scheduling.  This
 // mode never adds floats atomically: every particle writes its P2G source
 // record (stencil fractions, m v, m C, -dt V tau, m) and the id of its base
-// node; a stable radix sort groups the records by base node; then each grid
+// node; a stable radix sort groups the records by base node (the key of a
+// particle whose stencil left the grid is the node count, which sorts last).
 // The records are copied into sorted order (k_det_permute), each record whole,
 // so a base node's records form one contiguous run.  One thread per run sums,
 // particle by particle in sorted order, the run's contributions to each of the
@@ -31,7 +32,6 @@ struct SrcPlanes {
     // a record of the sorted copy: COUNT floats padded to whole float4s
     static constexpr int STRIDE = (COUNT + 3) / 4 * 4;
 };
-
 
 template <int D>
 __global__ void __launch_bounds__(128) k_det_source(ParticleBuf pb, long long n, const GroupParams* __restrict__ groups,
