@@ -830,8 +830,12 @@ void Engine::enqueue_rebin(int from, bool in_loop) {
     cudaMemsetAsync(counters + CNT_CHUNKS, 0, kMats * sizeof(int), stream);
     const unsigned nb = grid_blocks(n_particles, 256);
     if (n_particles > 0) {
-        auto k = dim == 3 ? (paged ? k_bin_count<3, true> : k_bin_count<3, false>)
-                          : (paged ? k_bin_count<2, true> : k_bin_count<2, false>);
+        // the particles arrive in the order the configuration's last binning gave them
+        const bool cm = kFusedCfgs[cfg].order == ORDER_CELL;
+        auto k = dim == 3 ? (paged ? (cm ? k_bin_count<3, true, true> : k_bin_count<3, true, false>)
+                                   : (cm ? k_bin_count<3, false, true> : k_bin_count<3, false, false>))
+                          : (paged ? (cm ? k_bin_count<2, true, true> : k_bin_count<2, true, false>)
+                                   : (cm ? k_bin_count<2, false, true> : k_bin_count<2, false, false>));
         k<<<nb, 256, 0, stream>>>(buf(from), n_particles, groups_d, scenes_d, mat_slots, keys[0], rank, cell_count,
                                   seg_count, pages);
         note_launch("k_bin_count");
@@ -839,10 +843,13 @@ void Engine::enqueue_rebin(int from, bool in_loop) {
     cub::DeviceScan::ExclusiveSum(scan_tmp, scan_tmp_bytes, seg_count, seg_start, (int)n_segs, stream);
     note_launch("cub::DeviceScan::ExclusiveSum");
     if (n_particles > 0) {
-        auto k = dim == 3 ? (paged ? k_bin_place<3, true> : k_bin_place<3, false>)
-                          : (paged ? k_bin_place<2, true> : k_bin_place<2, false>);
+        const bool cm = kFusedCfgs[cfg].order == ORDER_CELL;
+        auto k = dim == 3 ? (paged ? (cm ? k_bin_place<3, true, true> : k_bin_place<3, true, false>)
+                                   : (cm ? k_bin_place<3, false, true> : k_bin_place<3, false, false>))
+                          : (paged ? (cm ? k_bin_place<2, true, true> : k_bin_place<2, true, false>)
+                                   : (cm ? k_bin_place<2, false, true> : k_bin_place<2, false, false>));
         k<<<nb, 256, 0, stream>>>(buf(from), buf(to), n_particles, keys[0], rank, cell_count, seg_count, seg_start,
-                                  mat_slots, kFusedCfgs[cfg].order, in_loop ? 0 : 1, err_d, pages);
+                                  mat_slots, in_loop ? 0 : 1, err_d, pages);
         note_launch("k_bin_place");
     }
     if (dim == 3)

@@ -89,8 +89,14 @@ __device__ __forceinline__ void home_of(const SceneParams& sc, const float* x, l
 
 // Pass 1: home block b, cell c and material m of every particle, its rank
 // among the particles of (b, m, c) and the size of segment (b, m).
-// (PAGED: the cell counters of a block live at its physical block.)
-template <int D, bool PAGED>
+// (PAGED: the cell counters of a block live at its physical block.)  The
+// particles arrive in the last binning's order, so the lanes of a warp mostly
+// share a segment, and in cell-major order (CELL_MAJOR) runs of lanes share a
+// cell: those counter updates are aggregated per warp (one atomic per distinct
+// counter, each lane's rank the group's base plus its place among the group's
+// lanes).  In rank-major order the lanes sit in distinct cells and update
+// their cell counters one by one.
+template <int D, bool PAGED, bool CELL_MAJOR>
 __global__ void __launch_bounds__(256) k_bin_count(ParticleBuf pb, long long n, const GroupParams* __restrict__ groups,
                                                    const SceneParams* __restrict__ scenes, MatSlots ms,
                                                    unsigned long long* __restrict__ key, int* __restrict__ rank,
@@ -106,8 +112,21 @@ __global__ void __launch_bounds__(256) k_bin_count(ParticleBuf pb, long long n, 
     long long b;
     int c;
     home_of<D>(sc, x, b, c);
-    rank[i] = atomicAdd(&cell_count[(phys_block<PAGED>(gp, b) * ms.n + ms.s[g.type]) * 64 + c], 1);
-    atomicAdd(&seg_count[b * 4 + g.type], 1);
+    const unsigned act = __activemask();  // the lanes with a particle (the rest returned above)
+    const long long cell = (phys_block<PAGED>(gp, b) * ms.n + ms.s[g.type]) * 64 + c;
+    if constexpr (CELL_MAJOR) {
+        const unsigned lane_lt = (1u << (threadIdx.x & 31)) - 1u;
+        const unsigned in_cell = __match_any_sync(act, cell);
+        const int lead_c = __ffs(in_cell) - 1;
+        int base = 0;
+        if ((int)(threadIdx.x & 31) == lead_c) base = atomicAdd(&cell_count[cell], __popc(in_cell));
+        rank[i] = __shfl_sync(in_cell, base, lead_c) + __popc(in_cell & lane_lt);
+    } else {
+        rank[i] = atomicAdd(&cell_count[cell], 1);
+    }
+    const long long seg = b * 4 + g.type;
+    const unsigned in_seg = __match_any_sync(act, seg);
+    if ((int)(threadIdx.x & 31) == __ffs(in_seg) - 1) atomicAdd(&seg_count[seg], __popc(in_seg));
     key[i] = ((unsigned long long)b << 8) | ((unsigned long long)g.type << 6) | (unsigned long long)c;
 }
 
@@ -120,12 +139,12 @@ __global__ void __launch_bounds__(256) k_bin_count(ParticleBuf pb, long long n, 
 // the fused kernels never read them, they rewrite the v planes and rebuild
 // both on demand).  Ranks are exact, so the slots are a permutation of the
 // segment; a slot outside it (inconsistent counts) is reported, not written.
-template <int D, bool PAGED>
+template <int D, bool PAGED, bool CELL_MAJOR>
 __global__ void __launch_bounds__(256) k_bin_place(ParticleBuf src, ParticleBuf dst, long long n,
                                                    const unsigned long long* __restrict__ key,
                                                    const int* __restrict__ rank, const int* __restrict__ cell_count,
                                                    const int* __restrict__ seg_count,
-                                                   const int* __restrict__ seg_start, MatSlots ms, int cell_major,
+                                                   const int* __restrict__ seg_start, MatSlots ms,
                                                    int move_vc, unsigned* __restrict__ err, GridPages gp) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -134,19 +153,17 @@ __global__ void __launch_bounds__(256) k_bin_place(ParticleBuf src, ParticleBuf 
     const int m = (int)((k >> 6) & 3), c = (int)(k & 63);
     const int r = rank[i];
     const int4* cnt = reinterpret_cast<const int4*>(cell_count + (phys_block<PAGED>(gp, b) * ms.n + ms.s[m]) * 64);
-    int lower = 0, before = 0, cells_below = 0;
+    int off = CELL_MAJOR ? r : 0;
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
         const int4 v = cnt[q];
         const int nc[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
-            lower += min(nc[t], r);
-            before += (4 * q + t < c && nc[t] > r) ? 1 : 0;
-            cells_below += (4 * q + t < c) ? nc[t] : 0;
+            if constexpr (CELL_MAJOR) off += (4 * q + t < c) ? nc[t] : 0;  // the cells below, then the rank
+            else off += min(nc[t], r) + ((4 * q + t < c && nc[t] > r) ? 1 : 0);  // lower ranks, then rank r below c
         }
     }
-    const int off = cell_major ? cells_below + r : lower + before;
     const int seg = (int)(b * 4 + m);
     if (off < 0 || off >= seg_count[seg]) {
         atomicOr(err, ERR_BINNING);
